@@ -1,0 +1,266 @@
+"""Throughput of the p=619 production lease on B200 (focused candidate positions per second).
+
+Workload: 256-batch leases (1.6384e12 canonical v each, 16,384 subtiles of 1e8) of
+Config(619, 10^27, 3*10^27, A619, B619), starting at the seeded batch index
+random.Random(619003).randrange(0, 108298516 - 256 + 1); step k is the k-th consecutive lease
+after the warm-up leases.  One step = windows of both focuses from the resident wheel tables,
+per-v bounds, the fused bitset/128-bit kernel over every subtile, and the counters and outputs
+back on the host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own leases (replicas, no data exchange); rank 0 prints one
+JSON line.  ``--impl reference`` times the CPU restatement of the reference path (oracle/, with
+every host thread) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import random
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = 'focused candidate positions/s (p=619 production lease)'
+UNIT = 'positions/s'
+BATCHES_TOTAL = 108298517
+LEASE_BATCHES = 256
+OPS_PER_POSITION = 0.53071   # algorithmic 32-bit lane-ops per focused position (3W + 18S1 + 12T + 24Nv)
+
+
+def seeded_first_batch() -> int:
+    return random.Random(619003).randrange(0, BATCHES_TOTAL - 1 - LEASE_BATCHES + 1)
+
+
+def lease_bounds(index: int) -> tuple[int, int]:
+    from psuedocubes_b200.focus import B619
+    from psuedocubes_b200.optimized import BATCH_WIDTH, LEASE_WIDTH
+    first = (seeded_first_batch() * BATCH_WIDTH + index * LEASE_WIDTH) % (B619 - LEASE_WIDTH)
+    first -= first % BATCH_WIDTH
+    return first, first + LEASE_WIDTH
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device: int) -> None:
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self) -> 'ClockSampler':
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.device}', f'--query-gpu={self.QUERY}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self) -> None:
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(',')])
+
+    def __exit__(self, *exc) -> None:
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=['unsampled'])
+        sm = [float(r[1]) for r in self.rows if r[1].replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace('.', '').isdigit()]
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower() == 'active'})
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                    reasons=reasons, samples=len(self.rows))
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+        return rank, world, local, dist
+    return 0, 1, 0, None
+
+
+def max_over_ranks(dist, value: float, local: int) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f'cuda:{local}')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist) -> None:
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_sample(steps: int, warmup: int, batches: int = 16) -> dict:
+    """The oracle over `batches` batches of the first timed lease, every host thread."""
+    from oracle import pcube_oracle as O
+    g = O.Geometry(619, 10**27, 3 * 10**27, O.A619, O.B619)
+    fa, fb = O.OracleFocus(g, 'A'), O.OracleFocus(g, 'B')
+    first, _ = lease_bounds(warmup)
+    cores = os.cpu_count() or 1
+    positions, elapsed = 0, 0.0
+    for k in range(max(1, steps)):
+        start = first + k * batches * O.BATCH_WIDTH
+        t0 = time.perf_counter()
+        r = O.lease(g, fa, fb, start, start + batches * O.BATCH_WIDTH, workers=cores, threads_per_batch=1)
+        elapsed += time.perf_counter() - t0
+        positions += r['valid_focused_candidates']
+    return dict(value=positions / elapsed, unit=UNIT, cores=cores, kind='port',
+                sample=f'{batches} consecutive p=619 batches ({batches * 64} subtiles) per step, {max(1, steps)} steps, '
+                       f'C restatement of the window producer and masked matcher, {cores} threads',
+                seconds=elapsed, positions=positions)
+
+
+def run_reference(args) -> None:
+    rank, world, local, dist = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_sample(1, 0, batches=4)
+    sample = cpu_sample(args.steps, args.warmup, batches=8)
+    line = dict(metric=METRIC, value=sample['value'], unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=1000 * sample['seconds'] / max(1, args.steps),
+                higher_is_better=True, scaling='weak', vs_baseline=None, dtype='u64', data='synthetic',
+                impl='reference',
+                config=dict(workload='p=619 production lease, 256 batches x 64 subtiles x 1e8 v (bounded CPU sample)',
+                            p=619, lease_batches=LEASE_BATCHES, first_batch=seeded_first_batch()),
+                cpu_baseline=dict(value=sample['value'], unit=UNIT, cores=sample['cores'], kind=sample['kind'],
+                                  sample=sample['sample']),
+                e2e=dict(value=sample['value'], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import numpy as np
+    from psuedocubes_b200 import _native as N
+    from psuedocubes_b200.batch_experiment import MaskedMatcher
+    from psuedocubes_b200.focus import A619, B619, Config
+    from psuedocubes_b200.gpu import GPUFocus, MASK, Runtime
+    from psuedocubes_b200.optimized import PROFILE, compute_lease
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    runtime = Runtime(time.monotonic() + 7200, 16 * 1024**3, 0.5, device=local)
+    config = Config(619, 10**27, 3 * 10**27, A619, B619)
+    af, bf = (GPUFocus(runtime, f) for f in config.focuses())
+    matcher = MaskedMatcher(runtime, config)
+    width = PROFILE['tile_width']
+    nt = (LEASE_BATCHES * 64)
+    ng = len(matcher.filter_groups)
+    counts = np.zeros(nt * (ng + 3), dtype=np.uint64)
+    geometry = np.zeros(2 * nt, dtype=np.uint64)
+    cap = 1 << 16
+    records = np.zeros(2 * cap, dtype=np.uint64)
+    n_out = ctypes.c_uint64()
+    stats = N.Stats()
+    lib, ctx = runtime.lib, runtime.ctx
+    c = config
+
+    def step(index: int) -> tuple[int, dict]:
+        first, end = lease_bounds(index * world + rank)
+        runtime.call(lib.pc_run_lease(ctx, af.handle, bf.handle, matcher.filters.handle, ctypes.byref(matcher.tuning),
+                                      first, end, width, c.lo & MASK, c.lo >> 64, c.hi & MASK, c.hi >> 64, counts,
+                                      geometry, records, cap, ctypes.byref(n_out), ctypes.byref(stats)))
+        return int(counts.reshape(nt, ng + 3)[:, 0].sum()), stats.as_dict()
+
+    for k in range(args.warmup):
+        step(k)
+    barrier(dist)
+    runtime.synchronize()
+    positions, kernel_ms, launches, outputs = 0, 0.0, 0, 0
+    with ClockSampler(local) as clocks:
+        runtime.call(lib.pc_mark(ctx, 0))
+        for k in range(args.steps):
+            p, st = step(args.warmup + k)
+            positions += p
+            kernel_ms += st['kernel_ms']
+            launches += st['launches']
+            outputs += st['outputs']
+        runtime.call(lib.pc_mark(ctx, 1))
+        elapsed = ctypes.c_double()
+        runtime.call(lib.pc_elapsed(ctx, 0, 1, ctypes.byref(elapsed)))
+    seconds = max_over_ranks(dist, elapsed.value / 1000, local)
+    total_positions = positions * world   # every rank runs the same number of equal-size leases
+    # end to end through the public API: compute_lease with host assembly, verification, transcript
+    barrier(dist)
+    e2e_steps = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    e2e_positions = 0
+    for k in range(e2e_steps):
+        first, end = lease_bounds((args.warmup + args.steps + k) * world + rank)
+        result = compute_lease(matcher, af, bf, first, end)
+        e2e_positions += result['valid_focused_candidates']
+    e2e_seconds = max_over_ranks(dist, time.perf_counter() - t0, local)
+    d2h = counts.nbytes + geometry.nbytes + 16 + 16 * (outputs // max(1, args.steps))
+    if rank == 0:
+        clock = clocks.summary()
+        sm_mhz = clock['sm_max_mhz'] or 1965.0
+        peak = runtime.sm_count * 4 * 32 * sm_mhz * 1e6 / 1e12    # Tlane-op/s integer issue
+        achieved = OPS_PER_POSITION * positions / (kernel_ms / 1000) / 1e12 if kernel_ms else None
+        line = dict(metric=METRIC, value=total_positions / seconds, unit=UNIT, n_gpus=world, steps=args.steps,
+                    warmup=args.warmup, ms_per_step=1000 * seconds / args.steps, higher_is_better=True,
+                    scaling='weak', vs_baseline=None, dtype='u64', data='synthetic',
+                    config=dict(workload='p=619 production lease: 256 batches x 64 subtiles x 1e8 canonical v, '
+                                         'Config(619, 10^27, 3*10^27, A619, B619)',
+                                first_batch=seeded_first_batch(), lease_batches=LEASE_BATCHES, parallelism=f'replicas{world}',
+                                l2='inputs larger than L2 (resident wheel tables 208 MB, per-lease lists and bounds ~0.7 GB)'),
+                    roofline=dict(bound='int_alu', achieved=achieved, peak=peak, unit='Tlaneop/s',
+                                  frac=achieved / peak if achieved else None, traffic=None,
+                                  kernel='k_match (fused bitset + 128-bit filters)',
+                                  ops_per_position=OPS_PER_POSITION,
+                                  peak_basis=f'{runtime.sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz'),
+                    e2e=dict(value=e2e_positions * world / e2e_seconds, unit=UNIT, h2d_bytes_per_step=0,
+                             d2h_bytes_per_step=int(d2h), api='psuedocubes_b200.optimized.compute_lease'),
+                    gpu_launches=launches, clocks=clock,
+                    kernel_ms_per_step=kernel_ms / args.steps)
+        if world == 1 and not args.no_cpu:
+            line['cpu_baseline'] = {k: v for k, v in cpu_sample(1, args.warmup, batches=8).items()
+                                    if k in ('value', 'unit', 'cores', 'kind', 'sample')}
+        print(json.dumps(line), flush=True)
+    del af, bf, matcher
+    runtime.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__)
+    parser.add_argument('--gpus', type=int, default=1)
+    parser.add_argument('--steps', type=int, default=5)
+    parser.add_argument('--warmup', type=int, default=3)
+    parser.add_argument('--impl', choices=('ours', 'reference'), default='ours')
+    parser.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    args = parser.parse_args()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,189 @@
+// Shared device/host definitions of libpcube (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "../../include/pcube.h"
+
+#define PC_MAX_BITSET 8        // residual filters intersected as bitsets
+#define PC_MAX_RES 1024        // residual filters per (p, A, B)
+#define PC_MAX_WHEEL_T 6       // focus rings handled as wheel bitset rows
+
+// ------------------------------------------------------------------------------------------
+// context, errors, memory accounting
+
+struct pc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    cudaEvent_t marks[8] = {};
+    uint64_t cap = 0, in_use = 0, peak = 0;
+    int sm_count = 0, cc_major = 0, cc_minor = 0;
+    char name[256] = {};
+    std::string err;
+};
+
+struct pc_buf {
+    uint64_t *d = nullptr;
+    uint64_t n = 0;
+    uint64_t bytes = 0;
+};
+
+int pc_fail(pc_ctx *ctx, int code, const std::string &msg);
+int pc_cuda_fail(pc_ctx *ctx, cudaError_t e, const char *what);
+int pc_alloc(pc_ctx *ctx, void **ptr, uint64_t bytes);
+void pc_release(pc_ctx *ctx, void *ptr, uint64_t bytes);
+
+#define PC_CHECK(ctx, call)                                                   \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return pc_cuda_fail((ctx), e_, #call);         \
+    } while (0)
+
+#define PC_LAUNCHED(ctx, what)                                                \
+    do {                                                                      \
+        cudaError_t e_ = cudaGetLastError();                                  \
+        if (e_ != cudaSuccess) return pc_cuda_fail((ctx), e_, what);          \
+    } while (0)
+
+// RAII holder for device scratch owned by one call.
+struct Scratch {
+    pc_ctx *ctx;
+    std::vector<std::pair<void *, uint64_t>> items;
+    explicit Scratch(pc_ctx *c) : ctx(c) {}
+    ~Scratch() {
+        for (auto &it : items) pc_release(ctx, it.first, it.second);
+    }
+    template <class T>
+    int get(T **p, uint64_t count) {
+        uint64_t bytes = count * sizeof(T);
+        if (bytes == 0) bytes = 16;
+        void *q = nullptr;
+        int rc = pc_alloc(ctx, &q, bytes);
+        if (rc) return rc;
+        items.emplace_back(q, bytes);
+        *p = (T *)q;
+        return PC_OK;
+    }
+};
+
+__host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ uint64_t umax64(uint64_t a, uint64_t b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ int64_t imax64(int64_t a, int64_t b) { return a > b ? a : b; }
+
+// ------------------------------------------------------------------------------------------
+// 128-bit unsigned arithmetic in two 64-bit limbs (add.cc/addc and sub.cc/subc carry chains)
+
+struct u128 {
+    uint64_t lo, hi;
+};
+
+__device__ __forceinline__ u128 mul_wide(uint64_t a, uint64_t b) {
+    u128 r;
+    r.lo = a * b;
+    r.hi = __umul64hi(a, b);
+    return r;
+}
+
+__device__ __forceinline__ u128 add128(u128 a, u128 b) {
+    u128 r;
+    asm("add.cc.u64 %0, %2, %4;\n\taddc.u64 %1, %3, %5;"
+        : "=l"(r.lo), "=l"(r.hi)
+        : "l"(a.lo), "l"(a.hi), "l"(b.lo), "l"(b.hi));
+    return r;
+}
+
+__device__ __forceinline__ u128 sub128(u128 a, u128 b) {
+    u128 r;
+    asm("sub.cc.u64 %0, %2, %4;\n\tsubc.u64 %1, %3, %5;"
+        : "=l"(r.lo), "=l"(r.hi)
+        : "l"(a.lo), "l"(a.hi), "l"(b.lo), "l"(b.hi));
+    return r;
+}
+
+__device__ __forceinline__ bool less128(u128 a, u128 b) {
+    return a.hi < b.hi || (a.hi == b.hi && a.lo < b.lo);
+}
+
+// ------------------------------------------------------------------------------------------
+// Remainders by small odd or even moduli q < 2^16 without a hardware divide.
+//
+// fastmod32: Lemire, Kaser and Kurz, "Faster Remainder by Direct Computation" (2019): with
+// c = floor((2^64 - 1) / q) + 1, x mod q = floor(((c * x) mod 2^64) * q / 2^64) for every 32-bit x.
+//
+// A 128-bit value is folded first: with 16-bit limbs h_k and r_k = 2^(16k) mod q,
+// sum h_k r_k < 8 * 2^16 * 2^16 = 2^35 when q < 2^16; limbs are folded in two halves so each
+// partial sum stays below 2^32 for q < 2^13 (residual primes are far smaller).
+
+struct ModQ {
+    uint32_t q;
+    uint32_t r16[7];   // 2^(16k) mod q, k = 1..7
+    uint64_t c;        // fastmod constant
+};
+
+__host__ __device__ __forceinline__ uint64_t fastmod_constant(uint32_t q) {
+    return UINT64_C(0xFFFFFFFFFFFFFFFF) / q + 1;
+}
+
+__device__ __forceinline__ uint32_t fastmod32(uint32_t x, uint64_t c, uint32_t q) {
+    uint64_t low = c * x;
+    return (uint32_t)__umul64hi(low, q);
+}
+
+// x mod q for 64-bit x, q < 2^13 (r16 from a ModQ).
+__device__ __forceinline__ uint32_t mod64(uint64_t x, const ModQ &m) {
+    uint32_t w0 = (uint32_t)x, w1 = (uint32_t)(x >> 32);
+    uint32_t t = (w0 & 0xffffu) + (w0 >> 16) * m.r16[0] + (w1 & 0xffffu) * m.r16[1] + (w1 >> 16) * m.r16[2];
+    return fastmod32(t, m.c, m.q);
+}
+
+// x mod q for 128-bit x, q < 2^13.
+__device__ __forceinline__ uint32_t mod128(u128 x, const ModQ &m) {
+    uint32_t w0 = (uint32_t)x.lo, w1 = (uint32_t)(x.lo >> 32), w2 = (uint32_t)x.hi, w3 = (uint32_t)(x.hi >> 32);
+    uint32_t t0 = (w0 & 0xffffu) + (w0 >> 16) * m.r16[0] + (w1 & 0xffffu) * m.r16[1] + (w1 >> 16) * m.r16[2];
+    uint32_t t1 = (w2 & 0xffffu) * m.r16[3] + (w2 >> 16) * m.r16[4] + (w3 & 0xffffu) * m.r16[5] + (w3 >> 16) * m.r16[6];
+    return fastmod32(fastmod32(t0, m.c, m.q) + fastmod32(t1, m.c, m.q), m.c, m.q);
+}
+
+inline ModQ make_modq(uint32_t q) {
+    ModQ m{};
+    m.q = q;
+    uint64_t r = 1;
+    for (int k = 0; k < 7; ++k) {
+        r = (r << 16) % q;
+        m.r16[k] = (uint32_t)r;
+    }
+    m.c = fastmod_constant(q);
+    return m;
+}
+
+// Bits [n, 32) cleared for n in [0, 32]; PTX shl clamps shift counts >= 32 to a zero result.
+__device__ __forceinline__ uint32_t low_bits(uint32_t n) {
+    uint32_t r;
+    asm("shl.b32 %0, %1, %2;" : "=r"(r) : "r"(0xffffffffu), "r"(n));
+    return ~r;
+}
+
+// ------------------------------------------------------------------------------------------
+// 32x32 bit-matrix transpose across a warp: lane l holds row l (bit i = column i) on entry and
+// column l on exit.  Five exchange rounds of the off-diagonal blocks.
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane) {
+#pragma unroll
+    for (int j = 16; j >= 1; j >>= 1) {
+        const uint32_t hm = j == 16 ? 0xffff0000u : j == 8 ? 0xff00ff00u : j == 4 ? 0xf0f0f0f0u
+                          : j == 2 ? 0xccccccccu : 0xaaaaaaaau;
+        uint32_t p = __shfl_xor_sync(0xffffffffu, x, j);
+        bool upper = lane & j;
+        uint32_t keep = upper ? hm : ~hm;
+        uint32_t moved = upper ? (p >> j) : (p << j);
+        x = (x & keep) | (moved & ~keep);
+    }
+    return x;
+}
+
+// ------------------------------------------------------------------------------------------
+// internal host helpers shared across translation units
+
+int pc_exclusive_scan_u64(pc_ctx *ctx, const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total_dev);

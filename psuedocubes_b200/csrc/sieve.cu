@@ -1,0 +1,942 @@
+// Stages 2 and 3: residue-bitset intersection and exact 128-bit later filters.
+//
+// Layout.  The sorted u list is cut into blocks of K words (32 u per word).  A work item is one
+// u block and a run of consecutive v rows whose exact u interval meets the block.  The CTA that
+// owns an item builds, in shared memory, the residue rows of the first NB residual filters for
+// its block (row r of filter q, bit i <=> allowed_q[(u_i B - r A) mod q]) and then streams its v
+// rows: each v reads the K-word rows selected by v mod q with 128-bit loads, ANDs them, counts
+// the group survivors by popcount, and constructs x = uB - vA only for the bits that survive
+// every bitset filter.  Those are tested exactly against the remaining filters in 128-bit
+// arithmetic.
+//
+// Rows are stored as 16-byte units with the unit index XOR-swizzled by the row index, so the
+// transposing writer (32 rows, one unit each) and the readers (one row, consecutive units) both
+// touch all banks once per wavefront.
+#include "common.cuh"
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+struct FiltConst {
+    ModQ m;
+    uint32_t tab_off;   // word offset of the packed allowed bitmap
+    uint32_t pad;
+};
+
+struct pc_filters {
+    uint64_t A = 0, B = 0;
+    uint32_t nres = 0, ng = 0;
+    std::vector<uint32_t> primes;
+    FiltConst *d_fc = nullptr;
+    uint32_t *d_bits = nullptr;
+    uint32_t *d_pat = nullptr;       // swizzle-free RR patterns of the first filters (PATW words each)
+    uint64_t fc_bytes = 0, bits_bytes = 0, pat_bytes = 0;
+    uint32_t nbmax = 0;              // filters usable as bitset rows
+    uint32_t ainvb[PC_MAX_BITSET] = {};
+    uint32_t rows_sum[PC_MAX_BITSET + 1] = {};   // prefix sums of q over the first filters
+};
+
+namespace {
+
+constexpr int PATW = 136;            // pattern words per bitset filter (q <= 2047)
+constexpr int TMAX_DEFAULT = 64;     // subtile counter slots per CTA
+
+struct __align__(16) VRec {
+    uint32_t left, right, tile, pad;
+    uint16_t row[8];                 // row index (row0 + v mod q) of each bitset filter
+};
+
+struct MatchArgs {
+    const uint64_t *us;
+    const uint64_t *vs;
+    const VRec *rec;
+    uint64_t nu, nv;
+    uint64_t A, B;
+    u128 lo, hi;
+    uint32_t nres, ng, nb;
+    uint32_t tmax;
+    const FiltConst *fc;
+    const uint32_t *bits;
+    const uint32_t *pat;
+    uint32_t q[PC_MAX_BITSET];
+    uint32_t row0[PC_MAX_BITSET];
+    uint32_t ainvb[PC_MAX_BITSET];
+    ModQ mq[PC_MAX_BITSET];
+    uint32_t total_rows;
+    uint64_t *counts;                // ntiles x (ng+3)
+    uint64_t *out;
+    uint64_t out_cap;
+    unsigned long long *n_out;
+    uint32_t ntiles;
+    const uint2 *bv;                 // per u block: v index range
+    const uint64_t *item_prefix;     // nblocks + 1
+    uint64_t nblocks;
+    const uint64_t *vchunk;          // device scalar
+};
+
+// first j with us[j] * B > key
+__device__ __forceinline__ uint64_t count_le(const uint64_t *__restrict__ us, uint64_t n, uint64_t B, u128 key) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        if (less128(key, mul_wide(__ldg(us + mid), B))) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint64_t lower_bound64(const uint64_t *__restrict__ a, uint64_t n, uint64_t key) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        if (__ldg(a + mid) < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint64_t tile_of(uint64_t v, uint64_t v_first, uint64_t width) {
+    uint64_t d = v - v_first;
+    uint64_t t = (uint64_t)((double)d / (double)width);
+    while (t * width > d) --t;
+    while ((t + 1) * width <= d) ++t;
+    return t;
+}
+
+struct PrepArgs {
+    const uint64_t *us;
+    const uint64_t *vs;
+    uint64_t nu, nv, A, B;
+    u128 lo, hi;
+    uint64_t v_first, width;
+    uint32_t ntiles, nb, ng;
+    uint32_t q[PC_MAX_BITSET];
+    uint32_t row0[PC_MAX_BITSET];
+    ModQ mq[PC_MAX_BITSET];
+    VRec *rec;
+    uint64_t *counts;
+    unsigned long long *bad;
+};
+
+// Per v row: exact u interval as list indices (batch_experiment.py:209-215), subtile, bitset
+// row indices, and focused-position count of the subtile (popcount of the range masks there).
+__global__ void k_vprep(const PrepArgs a) {
+    uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t tile = UINT64_MAX, pop0 = 0;
+    if (j < a.nv) {
+        uint64_t v = a.vs[j];
+        u128 shift = mul_wide(v, a.A);
+        uint64_t left = count_le(a.us, a.nu, a.B, add128(shift, a.lo));
+        uint64_t right = count_le(a.us, a.nu, a.B, add128(shift, a.hi));
+        if (right < left) right = left;
+        if (v < a.v_first) {
+            atomicAdd(a.bad, 1ull);
+        } else {
+            tile = tile_of(v, a.v_first, a.width);
+            if (tile >= a.ntiles) {
+                atomicAdd(a.bad, 1ull);
+                tile = UINT64_MAX;
+            }
+        }
+        VRec r;
+        r.left = (uint32_t)left;
+        r.right = (uint32_t)right;
+        r.tile = tile == UINT64_MAX ? 0u : (uint32_t)tile;
+        r.pad = 0;
+#pragma unroll
+        for (int f = 0; f < PC_MAX_BITSET; ++f)
+            r.row[f] = f < (int)a.nb ? (uint16_t)(a.row0[f] + mod64(v, a.mq[f])) : (uint16_t)0;
+        a.rec[j] = r;
+        pop0 = right - left;
+    }
+    // warp-aggregated subtile sums (consecutive v rows mostly share a subtile)
+    uint64_t t0 = __shfl_sync(0xffffffffu, tile, 0);
+    bool same = __all_sync(0xffffffffu, tile == t0 || tile == UINT64_MAX);
+    if (same) {
+        uint64_t s = pop0;
+#pragma unroll
+        for (int d = 16; d; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
+        if (lane == 0 && t0 != UINT64_MAX && s) atomicAdd((unsigned long long *)&a.counts[t0 * (a.ng + 3)], (unsigned long long)s);
+    } else if (tile != UINT64_MAX && pop0) {
+        atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3)], (unsigned long long)pop0);
+    }
+}
+
+// Per subtile: u count and v count of its envelope (searchsorted bounds of
+// batch_experiment.py:37-43, as list-independent differences).
+__global__ void k_geometry(const uint64_t *__restrict__ us, uint64_t nu, const uint64_t *__restrict__ vs, uint64_t nv,
+                           uint64_t A, uint64_t B, u128 lo, u128 hi, uint64_t v_first, uint64_t width,
+                           uint64_t v_end, uint32_t ntiles, uint64_t *__restrict__ geometry) {
+    uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s >= ntiles) return;
+    uint64_t first = v_first + s * width;
+    uint64_t end = min(first + width, v_end);
+    uint64_t ua = count_le(us, nu, B, add128(mul_wide(first, A), lo));
+    uint64_t ub = count_le(us, nu, B, add128(mul_wide(end - 1, A), hi));
+    uint64_t va = lower_bound64(vs, nv, first), vb = lower_bound64(vs, nv, end);
+    geometry[2 * s] = ub > ua ? ub - ua : 0;
+    geometry[2 * s + 1] = vb - va;
+}
+
+// Per u block of UB entries: [va, vb) of v rows whose [left, right) meets the block.
+__global__ void k_blocks(const VRec *__restrict__ rec, uint64_t nv, uint64_t nu, uint32_t UB, uint64_t nblocks,
+                         uint2 *__restrict__ bv, uint64_t *__restrict__ pieces) {
+    uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    uint64_t start = b * UB, stop = umin64(nu, start + UB);
+    uint64_t lo = 0, hi = nv;                       // first j with right > start
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        if (rec[mid].right > start) hi = mid;
+        else lo = mid + 1;
+    }
+    uint64_t va = lo;
+    lo = va, hi = nv;                               // first j with left >= stop
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        if (rec[mid].left >= stop) hi = mid;
+        else lo = mid + 1;
+    }
+    uint64_t vb = lo;
+    bv[b] = make_uint2((uint32_t)va, (uint32_t)vb);
+    pieces[b] = vb > va ? vb - va : 0;
+}
+
+// v chunk per work item: fixed, or total pieces / target items (at least 64, at most 2^20).
+__global__ void k_chunk(const uint64_t *__restrict__ total_pieces, uint64_t fixed_chunk, uint64_t target_items,
+                        uint64_t *__restrict__ vchunk) {
+    uint64_t c = fixed_chunk;
+    if (!c) c = umax64((*total_pieces + target_items - 1) / umax64(1, target_items), 64);
+    *vchunk = umin64(c, UINT64_C(1) << 20);
+}
+
+__global__ void k_item_counts(const uint64_t *__restrict__ pieces, uint64_t nblocks,
+                              const uint64_t *__restrict__ vchunk, uint64_t *__restrict__ items) {
+    uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    uint64_t c = *vchunk;
+    items[b] = (pieces[b] + c - 1) / c;
+}
+
+// ------------------------------------------------------------------------------------------
+// the fused kernel
+
+template <int K>
+struct Geo {
+    static constexpr int U = K / 4;                      // 16-byte units per row
+    static constexpr int UB = K * 32;                    // u entries per block
+    static constexpr int SWS = U == 4 ? 1 : 0;           // swizzle shift
+    __device__ static __forceinline__ uint32_t unit(uint32_t row, uint32_t c) {
+        return row * U + (c ^ ((row >> SWS) & (U - 1)));
+    }
+};
+
+template <int NB, int K>
+__device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, const uint64_t *__restrict__ us_s,
+                           const uint32_t *__restrict__ pat_s, uint64_t block_u0, uint32_t lane, uint32_t warp,
+                           uint32_t nwarps) {
+    using G = Geo<K>;
+    // a warp builds all q rows of one filter for one 16-byte unit (4 words = 128 u)
+    for (uint32_t pair = warp; pair < NB * G::U; pair += nwarps) {
+        uint32_t f = pair / G::U, c = pair % G::U;
+        const uint32_t q = a.q[f];
+        uint32_t t[4];
+        bool valid[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint32_t local = (c * 4 + k) * 32 + lane;
+            valid[k] = block_u0 + local < a.nu;
+            uint32_t um = valid[k] ? mod64(us_s[local], a.mq[f]) : 0;
+            t[k] = fastmod32(um * a.ainvb[f], a.mq[f].c, q);
+        }
+        const uint32_t *p = pat_s + f * PATW;
+        for (uint32_t g = 0; g * 32 < q; ++g) {
+            uint32_t w[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                uint32_t st = 32 * g + q - t[k];
+                uint32_t col = __funnelshift_r(p[st >> 5], p[(st >> 5) + 1], st & 31);
+                w[k] = transpose32(valid[k] ? col : 0u, lane);
+            }
+            uint32_t r = 32 * g + lane;
+            if (r < q) {
+                uint32_t row = a.row0[f] + r;
+                rows[G::unit(row, c)] = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+    }
+}
+
+// Arithmetic filters idx = first..nres-1 on a survivor; group counters into shared slots.
+// Returns true if x passes every filter.
+__device__ __forceinline__ bool later_filters(const MatchArgs &a, u128 x, uint32_t first, uint32_t *cnt_slot,
+                                              uint64_t tile) {
+    for (uint32_t idx = first; idx < a.nres; ++idx) {
+        const FiltConst fc = a.fc[idx];
+        uint32_t m = mod128(x, fc.m);
+        if (!((__ldg(a.bits + fc.tab_off + (m >> 5)) >> (m & 31)) & 1u)) return false;
+        if ((idx & 3) == 3 || idx + 1 == a.nres) {
+            uint32_t g = idx / 4 + 1;
+            if (cnt_slot) atomicAdd(cnt_slot + g, 1u);
+            else atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], 1ull);
+        }
+    }
+    return true;
+}
+
+template <int NB, int K>
+__global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
+    using G = Geo<K>;
+    constexpr int WPL = 4;
+    constexpr int LPV = K / WPL;          // lanes per v row
+    constexpr int VPW = 32 / LPV;         // v rows per warp step
+    extern __shared__ uint4 smem[];
+    uint4 *rows = smem;
+    uint64_t *us_s = (uint64_t *)(rows + (size_t)a.total_rows * G::U);
+    uint32_t *pat_s = (uint32_t *)(us_s + G::UB);
+    uint32_t *cnt_s = pat_s + NB * PATW;                  // tmax x (ng+2): groups 1..ng, outputs
+    const uint32_t stride = a.ng + 2;
+
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t gsel = lane / LPV, sub = lane % LPV;
+
+    for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = a.pat[i];
+
+    const uint64_t n_items = a.item_prefix[a.nblocks];
+    const uint64_t vch = *a.vchunk;
+    const uint64_t i0 = n_items * blockIdx.x / gridDim.x, i1 = n_items * (blockIdx.x + 1) / gridDim.x;
+    uint64_t cur = UINT64_MAX, bsearch = 0;
+    if (i0 < i1) {                                        // block of the first item: last b with prefix[b] <= i0
+        uint64_t lo = 0, hi = a.nblocks;
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) / 2;
+            if (a.item_prefix[mid] <= i0) lo = mid;
+            else hi = mid;
+        }
+        bsearch = lo;
+    }
+    const bool c2_live = NB == 8 || (NB > 4 && NB == (int)a.nres);
+
+    for (uint64_t it = i0; it < i1; ++it) {
+        while (a.item_prefix[bsearch + 1] <= it) ++bsearch;  // items are visited in order
+        const uint64_t b = bsearch;
+        const uint2 range = a.bv[b];
+        const uint64_t va = range.x + (it - a.item_prefix[b]) * vch;
+        const uint64_t vb = umin64(range.y, va + vch);
+        const uint64_t block_u0 = b * G::UB;
+        __syncthreads();                                  // previous item finished with smem
+        if (b != cur) {
+            for (uint32_t k = threadIdx.x; k < G::UB; k += blockDim.x)
+                us_s[k] = block_u0 + k < a.nu ? a.us[block_u0 + k] : 0;
+            __syncthreads();
+            build_rows<NB, K>(a, rows, us_s, pat_s, block_u0, lane, warp, nwarps);
+            cur = b;
+        }
+        for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) cnt_s[k] = 0;
+        __syncthreads();
+        const uint32_t tile_base = a.rec[va].tile;
+
+        uint32_t c1 = 0, c2 = 0, ctile = UINT32_MAX;
+        auto flush = [&]() {
+            if (ctile == UINT32_MAX || (c1 == 0 && c2 == 0)) return;
+            uint32_t slot = ctile - tile_base;
+            if (slot < a.tmax) {
+                if (c1) atomicAdd(cnt_s + slot * stride + 1, c1);
+                if (c2) atomicAdd(cnt_s + slot * stride + 2, c2);
+            } else {
+                if (c1) atomicAdd((unsigned long long *)&a.counts[(uint64_t)ctile * (a.ng + 3) + 1], (unsigned long long)c1);
+                if (c2) atomicAdd((unsigned long long *)&a.counts[(uint64_t)ctile * (a.ng + 3) + 2], (unsigned long long)c2);
+            }
+            c1 = c2 = 0;
+        };
+
+        for (uint64_t v0 = va + (uint64_t)warp * VPW; v0 < vb; v0 += (uint64_t)nwarps * VPW) {
+            const uint64_t vi = v0 + gsel;
+            const bool active = vi < vb;
+            VRec r;
+            if (active) r = a.rec[vi];
+            else {
+                r.left = r.right = 0;
+                r.tile = ctile;
+#pragma unroll
+                for (int f = 0; f < 8; ++f) r.row[f] = a.row0[0];
+            }
+            int64_t s = (int64_t)r.left - (int64_t)block_u0, e = (int64_t)r.right - (int64_t)block_u0;
+            s = imax64(s, 0);
+            e = imin64(e, G::UB);
+            if (!active || e < s) e = s;
+            const int32_t lb = sub * WPL * 32;
+            int32_t ls = (int32_t)imin64(imax64(s - lb, 0), WPL * 32);
+            int32_t le = (int32_t)imin64(imax64(e - lb, 0), WPL * 32);
+
+            uint4 acc = rows[G::unit(r.row[0], sub)];
+            uint4 acc4;
+#pragma unroll
+            for (int f = 1; f < NB; ++f) {
+                if (f == 4) acc4 = acc;
+                uint4 x = rows[G::unit(r.row[f], sub)];
+                acc.x &= x.x;
+                acc.y &= x.y;
+                acc.z &= x.z;
+                acc.w &= x.w;
+            }
+            if (NB <= 4) acc4 = acc;
+            uint32_t w4[4] = {acc4.x, acc4.y, acc4.z, acc4.w};
+            uint32_t wn[4] = {acc.x, acc.y, acc.z, acc.w};
+            if (ls > 0 || le < WPL * 32) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    int32_t a0 = min(max(ls - 32 * k, 0), 32), a1 = min(max(le - 32 * k, 0), 32);
+                    uint32_t m = low_bits((uint32_t)a1) & ~low_bits((uint32_t)a0);
+                    w4[k] &= m;
+                    wn[k] &= m;
+                }
+            }
+            if (active && r.tile != ctile) {
+                flush();
+                ctile = r.tile;
+            }
+            c1 += __popc(w4[0]) + __popc(w4[1]) + __popc(w4[2]) + __popc(w4[3]);
+            if (c2_live) c2 += __popc(wn[0]) + __popc(wn[1]) + __popc(wn[2]) + __popc(wn[3]);
+
+            bool more = (wn[0] | wn[1] | wn[2] | wn[3]) != 0;
+            if (__any_sync(0xffffffffu, more)) {
+                const uint64_t v = active ? a.vs[vi] : 0;
+                const u128 shift = mul_wide(v, a.A);
+                const uint32_t slot = r.tile - tile_base;
+                uint32_t *cs = slot < a.tmax ? cnt_s + slot * stride : nullptr;
+                while (__any_sync(0xffffffffu, more)) {
+                    if (more) {
+                        uint32_t local = 0;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            if (wn[k]) {
+                                uint32_t bit = __ffs(wn[k]) - 1;
+                                wn[k] &= wn[k] - 1;
+                                local = lb + 32 * k + bit;
+                                break;
+                            }
+                        }
+                        more = (wn[0] | wn[1] | wn[2] | wn[3]) != 0;
+                        const u128 pos = mul_wide(us_s[local], a.B);
+                        if (less128(pos, shift)) {
+                            atomicAdd((unsigned long long *)&a.counts[(uint64_t)r.tile * (a.ng + 3) + a.ng + 2], 1ull);
+                        } else {
+                            const u128 x = sub128(pos, shift);
+                            if (later_filters(a, x, NB, cs, r.tile)) {
+                                if (cs) atomicAdd(cs + a.ng + 1, 1u);
+                                else atomicAdd((unsigned long long *)&a.counts[(uint64_t)r.tile * (a.ng + 3) + a.ng + 1], 1ull);
+                                unsigned long long o = atomicAdd(a.n_out, 1ull);
+                                if (o < a.out_cap) {
+                                    a.out[2 * o] = x.lo;
+                                    a.out[2 * o + 1] = x.hi | ((uint64_t)r.tile << 32);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        flush();
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) {
+            uint32_t c = cnt_s[k];
+            if (c) {
+                uint32_t slot = k / stride, g = k % stride;
+                uint64_t tile = (uint64_t)tile_base + slot;
+                if (tile < a.ntiles)
+                    atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], (unsigned long long)c);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// plain per-position matcher (pseudocube/gpu.py:147-182): warp per v row, lanes over u
+
+struct PlainArgs {
+    const uint64_t *us;
+    const uint64_t *vs;
+    uint64_t nu, nv, A, B;
+    u128 lo, hi;
+    uint32_t nres, ng;
+    const FiltConst *fc;
+    const uint32_t *bits;
+    uint64_t *counts;
+    uint64_t *out;
+    uint64_t out_cap;
+};
+
+__global__ void __launch_bounds__(256) k_plain(const PlainArgs a) {
+    __shared__ unsigned long long cnt[PC_MAX_RES / 4 + 4];
+    for (uint32_t k = threadIdx.x; k < a.ng + 3; k += blockDim.x) cnt[k] = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    unsigned long long c0 = 0;
+    for (uint64_t j = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; j < a.nv; j += warps) {
+        const u128 shift = mul_wide(a.vs[j], a.A), upper = add128(shift, a.hi);
+        const uint64_t left = count_le(a.us, a.nu, a.B, add128(shift, a.lo));
+        for (uint64_t i = left + lane; i < a.nu; i += 32) {
+            const u128 pos = mul_wide(a.us[i], a.B);
+            if (less128(upper, pos)) break;
+            if (less128(pos, shift)) {
+                atomicAdd(&cnt[a.ng + 2], 1ull);
+                continue;
+            }
+            const u128 x = sub128(pos, shift);
+            ++c0;
+            bool ok = true;
+            for (uint32_t idx = 0; idx < a.nres; ++idx) {
+                const FiltConst fc = a.fc[idx];
+                uint32_t m = mod128(x, fc.m);
+                if (!((__ldg(a.bits + fc.tab_off + (m >> 5)) >> (m & 31)) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                if ((idx & 3) == 3 || idx + 1 == a.nres) atomicAdd(&cnt[idx / 4 + 1], 1ull);
+            }
+            if (!ok) continue;
+            unsigned long long slot = atomicAdd((unsigned long long *)&a.counts[a.ng + 1], 1ull);
+            if (slot < a.out_cap) {
+                a.out[2 * slot] = x.lo;
+                a.out[2 * slot + 1] = x.hi;
+            }
+        }
+    }
+    atomicAdd(&cnt[0], c0);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < a.ng + 3; k += blockDim.x)
+        if (k != a.ng + 1 && cnt[k]) atomicAdd((unsigned long long *)&a.counts[k], cnt[k]);
+}
+
+template <int NB, int K>
+int launch_match_t(pc_ctx *ctx, const MatchArgs &a, size_t smem, int threads, int grid) {
+    auto kern = k_match<NB, K>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return pc_cuda_fail(ctx, e, "match smem attribute");
+    kern<<<grid, threads, smem, ctx->stream>>>(a);
+    PC_LAUNCHED(ctx, "match");
+    return PC_OK;
+}
+
+template <int K>
+int launch_match_k(pc_ctx *ctx, const MatchArgs &a, size_t smem, int threads, int grid) {
+    switch (a.nb) {
+        case 1: return launch_match_t<1, K>(ctx, a, smem, threads, grid);
+        case 2: return launch_match_t<2, K>(ctx, a, smem, threads, grid);
+        case 3: return launch_match_t<3, K>(ctx, a, smem, threads, grid);
+        case 4: return launch_match_t<4, K>(ctx, a, smem, threads, grid);
+        case 5: return launch_match_t<5, K>(ctx, a, smem, threads, grid);
+        case 6: return launch_match_t<6, K>(ctx, a, smem, threads, grid);
+        case 7: return launch_match_t<7, K>(ctx, a, smem, threads, grid);
+        case 8: return launch_match_t<8, K>(ctx, a, smem, threads, grid);
+    }
+    return pc_fail(ctx, PC_INVALID, "unsupported bitset filter count");
+}
+
+uint32_t inv_mod(uint32_t a, uint32_t q) {
+    int64_t t = 0, nt = 1, r = q, nr = a % q;
+    while (nr) {
+        int64_t quo = r / nr, tmp;
+        tmp = t - quo * nt; t = nt; nt = tmp;
+        tmp = r - quo * nr; r = nr; nr = tmp;
+    }
+    if (r != 1) return 0;
+    return (uint32_t)(t < 0 ? t + q : t);
+}
+
+double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+}  // namespace
+
+extern "C" int pc_filters_create(pc_ctx *ctx, uint64_t A, uint64_t B, const uint32_t *primes, uint32_t nres,
+                                 const uint8_t *allowed, pc_filters **out) {
+    *out = nullptr;
+    if (nres == 0) return pc_fail(ctx, PC_INVALID, "bitset experiment requires at least one residual filter");
+    if (nres > PC_MAX_RES || A == 0 || B == 0) return pc_fail(ctx, PC_INVALID, "invalid residual filters");
+    pc_filters *f = new pc_filters();
+    f->A = A;
+    f->B = B;
+    f->nres = nres;
+    f->ng = (nres + 3) / 4;
+    f->primes.assign(primes, primes + nres);
+    std::vector<FiltConst> fc(nres);
+    std::vector<uint32_t> bits;
+    uint64_t off = 0;
+    for (uint32_t i = 0; i < nres; ++i) {
+        uint32_t q = primes[i];
+        if (q < 2 || q >= 8192 || A % q == 0 || B % q == 0) {
+            delete f;
+            return pc_fail(ctx, PC_INVALID, "residual modulus must be in [2, 8192) and coprime to A and B");
+        }
+        fc[i].m = make_modq(q);
+        fc[i].tab_off = (uint32_t)bits.size();
+        std::vector<uint32_t> w((q + 31) / 32, 0);
+        for (uint32_t r = 0; r < q; ++r)
+            if (allowed[off + r]) w[r / 32] |= 1u << (r % 32);
+        bits.insert(bits.end(), w.begin(), w.end());
+        off += q;
+    }
+    // patterns of the first filters: RR[j] = S'[(-j) mod q] with S'[k] = allowed[(A k) mod q]
+    f->nbmax = std::min<uint32_t>(nres, PC_MAX_BITSET);
+    std::vector<uint32_t> pat((size_t)PC_MAX_BITSET * PATW, 0);
+    uint64_t aoff = 0;
+    for (uint32_t i = 0; i < f->nbmax; ++i) {
+        uint32_t q = primes[i];
+        if (q > 2047) {
+            f->nbmax = i;
+            break;
+        }
+        uint32_t a = (uint32_t)(A % q), b = (uint32_t)(B % q);
+        f->ainvb[i] = (uint32_t)((uint64_t)b * inv_mod(a, q) % q);
+        for (uint32_t j = 0; j < 2 * q + 64; ++j) {
+            uint32_t k = (q - j % q) % q;
+            uint32_t m = (uint32_t)((uint64_t)a * k % q);
+            if (allowed[aoff + m]) pat[(size_t)i * PATW + j / 32] |= 1u << (j % 32);
+        }
+        aoff += q;
+        f->rows_sum[i + 1] = f->rows_sum[i] + q;
+    }
+    if (f->nbmax < std::min<uint32_t>(nres, 4)) {
+        delete f;
+        return pc_fail(ctx, PC_INVALID, "first residual filters too large for bitset rows");
+    }
+    f->fc_bytes = nres * sizeof(FiltConst);
+    f->bits_bytes = bits.size() * 4;
+    f->pat_bytes = pat.size() * 4;
+    int rc = pc_alloc(ctx, (void **)&f->d_fc, f->fc_bytes);
+    if (!rc) rc = pc_alloc(ctx, (void **)&f->d_bits, f->bits_bytes);
+    if (!rc) rc = pc_alloc(ctx, (void **)&f->d_pat, f->pat_bytes);
+    if (rc) {
+        pc_filters_free(ctx, f);
+        return rc;
+    }
+    cudaMemcpyAsync(f->d_fc, fc.data(), f->fc_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(f->d_bits, bits.data(), f->bits_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(f->d_pat, pat.data(), f->pat_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        pc_filters_free(ctx, f);
+        return pc_cuda_fail(ctx, e, "filters upload");
+    }
+    *out = f;
+    return PC_OK;
+}
+
+extern "C" int pc_filters_free(pc_ctx *ctx, pc_filters *f) {
+    if (!f) return PC_OK;
+    pc_release(ctx, f->d_fc, f->fc_bytes);
+    pc_release(ctx, f->d_bits, f->bits_bytes);
+    pc_release(ctx, f->d_pat, f->pat_bytes);
+    delete f;
+    return PC_OK;
+}
+
+namespace {
+
+struct Tuned {
+    uint32_t nb, K, threads;
+    uint64_t v_chunk;
+};
+
+Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_t *smem_out, uint32_t *tmax_out) {
+    Tuned r{};
+    uint32_t nb_min = std::min<uint32_t>(f->nres, 4);
+    r.nb = t && t->bitset_filters ? t->bitset_filters : std::min<uint32_t>(f->nbmax, 6);
+    r.nb = std::max(nb_min, std::min(r.nb, f->nbmax));
+    r.K = t && t->block_words ? t->block_words : 32;
+    if (r.K != 16 && r.K != 32 && r.K != 64) r.K = 32;
+    r.threads = t && t->threads ? t->threads : 512;
+    if (r.threads != 256 && r.threads != 512) r.threads = 512;
+    r.v_chunk = t ? t->v_chunk : 0;
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+    if (optin <= 0) optin = 227 * 1024;
+    for (;;) {
+        size_t rows = (size_t)f->rows_sum[r.nb] * (r.K / 4) * 16;
+        size_t fixed = rows + (size_t)r.K * 32 * 8 + (size_t)r.nb * PATW * 4;
+        size_t per_slot = (size_t)(f->ng + 2) * 4;
+        if (fixed + per_slot * 4 <= (size_t)optin) {
+            uint32_t tmax = (uint32_t)std::min<size_t>(TMAX_DEFAULT, ((size_t)optin - fixed) / per_slot);
+            *tmax_out = tmax;
+            *smem_out = fixed + per_slot * tmax;
+            return r;
+        }
+        if (r.K > 16) r.K /= 2;
+        else if (r.nb > nb_min) r.nb--;
+        else {
+            *smem_out = 0;
+            return r;
+        }
+    }
+}
+
+struct BatchIO {
+    uint64_t *counts, *geometry, *out;
+    uint64_t out_cap, *n_out;
+    pc_stats *stats;
+};
+
+// Device part shared by pc_run_batch and pc_run_lease.
+int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const uint64_t *d_us, uint64_t nu,
+               const uint64_t *d_vs, uint64_t nv, u128 lo, u128 hi, uint64_t v_first, uint64_t width,
+               uint32_t ntiles, uint64_t v_end, const BatchIO &io, int launches0) {
+    if (nu >= (UINT64_C(1) << 32) || nv >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "focus list too long");
+    const uint32_t ng = f->ng, stride = ng + 3;
+    size_t smem = 0;
+    uint32_t tmax = 0;
+    Tuned tn = resolve_tuning(ctx, f, tuning, &smem, &tmax);
+    if (!smem) return pc_fail(ctx, PC_INVALID, "residual rows do not fit shared memory");
+    Scratch s(ctx);
+    uint64_t *d_counts, *d_geo, *d_out, *d_prefix, *d_vchunk, *d_pieces;
+    unsigned long long *d_nout, *d_bad;
+    VRec *d_rec;
+    uint2 *d_bv;
+    const uint32_t UB = tn.K * 32;
+    const uint64_t nblocks = (nu + UB - 1) / UB;
+    int rc = s.get(&d_counts, (uint64_t)ntiles * stride);
+    if (!rc) rc = s.get(&d_geo, 2 * (uint64_t)ntiles);
+    if (!rc) rc = s.get(&d_out, 2 * std::max<uint64_t>(1, io.out_cap));
+    if (!rc) rc = s.get(&d_nout, 2);
+    if (!rc) rc = s.get(&d_rec, std::max<uint64_t>(1, nv));
+    if (!rc) rc = s.get(&d_bv, std::max<uint64_t>(1, nblocks));
+    if (!rc) rc = s.get(&d_pieces, std::max<uint64_t>(1, nblocks));
+    if (!rc) rc = s.get(&d_prefix, nblocks + 1);
+    if (!rc) rc = s.get(&d_vchunk, 1);
+    if (rc) return rc;
+    d_bad = d_nout + 1;
+    cudaStream_t st = ctx->stream;
+    PC_CHECK(ctx, cudaMemsetAsync(d_counts, 0, (uint64_t)ntiles * stride * 8, st));
+    PC_CHECK(ctx, cudaMemsetAsync(d_nout, 0, 16, st));
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[0], st));
+    int launches = launches0;
+
+    PrepArgs pa{};
+    pa.us = d_us;
+    pa.vs = d_vs;
+    pa.nu = nu;
+    pa.nv = nv;
+    pa.A = f->A;
+    pa.B = f->B;
+    pa.lo = lo;
+    pa.hi = hi;
+    pa.v_first = v_first;
+    pa.width = width;
+    pa.ntiles = ntiles;
+    pa.nb = tn.nb;
+    pa.ng = ng;
+    for (uint32_t i = 0; i < tn.nb; ++i) {
+        pa.q[i] = f->primes[i];
+        pa.row0[i] = f->rows_sum[i];
+        pa.mq[i] = make_modq(f->primes[i]);
+    }
+    pa.rec = d_rec;
+    pa.counts = d_counts;
+    pa.bad = d_bad;
+    if (nv) {
+        k_vprep<<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(pa);
+        PC_LAUNCHED(ctx, "vprep");
+        ++launches;
+    }
+    k_geometry<<<(ntiles + 127) / 128, 128, 0, st>>>(d_us, nu, d_vs, nv, f->A, f->B, lo, hi, v_first, width, v_end,
+                                                      ntiles, d_geo);
+    PC_LAUNCHED(ctx, "geometry");
+    ++launches;
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], st));
+    bool run_match = nu && nv;
+    if (run_match) {
+        k_blocks<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_rec, nv, nu, UB, nblocks, d_bv, d_pieces);
+        PC_LAUNCHED(ctx, "blocks");
+        int grid = ctx->sm_count;
+        uint64_t *d_items, *d_tmp;
+        rc = s.get(&d_items, nblocks);
+        if (!rc) rc = s.get(&d_tmp, nblocks + 1);
+        if (!rc) rc = pc_exclusive_scan_u64(ctx, d_pieces, d_tmp, nblocks, d_tmp + nblocks);
+        if (rc) return rc;
+        k_chunk<<<1, 1, 0, st>>>(d_tmp + nblocks, tn.v_chunk, (uint64_t)grid * 4, d_vchunk);
+        PC_LAUNCHED(ctx, "chunk");
+        k_item_counts<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_pieces, nblocks, d_vchunk, d_items);
+        PC_LAUNCHED(ctx, "item counts");
+        rc = pc_exclusive_scan_u64(ctx, d_items, d_prefix, nblocks, d_prefix + nblocks);
+        if (rc) return rc;
+        launches += 7;
+        MatchArgs ma{};
+        ma.us = d_us;
+        ma.vs = d_vs;
+        ma.rec = d_rec;
+        ma.nu = nu;
+        ma.nv = nv;
+        ma.A = f->A;
+        ma.B = f->B;
+        ma.lo = lo;
+        ma.hi = hi;
+        ma.nres = f->nres;
+        ma.ng = ng;
+        ma.nb = tn.nb;
+        ma.tmax = tmax;
+        ma.fc = f->d_fc;
+        ma.bits = f->d_bits;
+        ma.pat = f->d_pat;
+        for (uint32_t i = 0; i < tn.nb; ++i) {
+            ma.q[i] = f->primes[i];
+            ma.row0[i] = f->rows_sum[i];
+            ma.ainvb[i] = f->ainvb[i];
+            ma.mq[i] = make_modq(f->primes[i]);
+        }
+        ma.total_rows = f->rows_sum[tn.nb];
+        ma.counts = d_counts;
+        ma.out = d_out;
+        ma.out_cap = io.out_cap;
+        ma.n_out = d_nout;
+        ma.ntiles = ntiles;
+        ma.bv = d_bv;
+        ma.item_prefix = d_prefix;
+        ma.nblocks = nblocks;
+        ma.vchunk = d_vchunk;
+        PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
+        if (tn.K == 16) rc = launch_match_k<16>(ctx, ma, smem, tn.threads, grid);
+        else if (tn.K == 32) rc = launch_match_k<32>(ctx, ma, smem, tn.threads, grid);
+        else rc = launch_match_k<64>(ctx, ma, smem, tn.threads, grid);
+        if (rc) return rc;
+        ++launches;
+        PC_CHECK(ctx, cudaEventRecord(ctx->ev[3], st));
+    }
+    unsigned long long host_nout[2] = {0, 0};
+    PC_CHECK(ctx, cudaMemcpyAsync(host_nout, d_nout, 16, cudaMemcpyDeviceToHost, st));
+    PC_CHECK(ctx, cudaMemcpyAsync(io.counts, d_counts, (uint64_t)ntiles * stride * 8, cudaMemcpyDeviceToHost, st));
+    PC_CHECK(ctx, cudaMemcpyAsync(io.geometry, d_geo, 2 * (uint64_t)ntiles * 8, cudaMemcpyDeviceToHost, st));
+    PC_CHECK(ctx, cudaStreamSynchronize(st));
+    uint64_t n = host_nout[0];
+    *io.n_out = n;
+    if (io.stats) {
+        io.stats->bounds_ms = elapsed_ms(ctx->ev[0], ctx->ev[1]);
+        io.stats->kernel_ms = run_match ? elapsed_ms(ctx->ev[2], ctx->ev[3]) : 0.0;
+        io.stats->outputs = n;
+        io.stats->launches = launches;
+    }
+    if (host_nout[1]) return pc_fail(ctx, PC_INVALID, "v row outside the subtile geometry");
+    if (n > io.out_cap) return pc_fail(ctx, PC_OVERFLOW, "output overflow; attempt cannot commit");
+    if (n) {
+        PC_CHECK(ctx, cudaMemcpyAsync(io.out, d_out, 2 * n * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, cudaStreamSynchronize(st));
+    }
+    for (uint32_t t = 0; t < ntiles; ++t)
+        if (io.counts[(uint64_t)t * stride + ng + 2]) return pc_fail(ctx, PC_ARITHMETIC, "unsigned underflow flagged");
+    return PC_OK;
+}
+
+}  // namespace
+
+int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, uint64_t cap, uint64_t **out,
+                   uint64_t *out_bytes, uint64_t *total_host, int *launches);
+
+extern "C" int pc_run_batch(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const pc_buf *us, uint64_t u_off,
+                            uint64_t nu, const pc_buf *vs, uint64_t v_off, uint64_t nv, uint64_t lo0, uint64_t lo1,
+                            uint64_t hi0, uint64_t hi1, uint64_t v_first, uint64_t width, uint32_t ntiles,
+                            uint64_t v_end, uint64_t *counts, uint64_t *geometry, uint64_t *out, uint64_t out_cap,
+                            uint64_t *n_out, pc_stats *stats) {
+    if (!f || !us || !vs || width == 0 || ntiles == 0) return pc_fail(ctx, PC_INVALID, "invalid batch arguments");
+    if (u_off > us->n || nu > us->n - u_off || v_off > vs->n || nv > vs->n - v_off)
+        return pc_fail(ctx, PC_INVALID, "focus list slice out of range");
+    if (v_end <= v_first || (v_end - v_first + width - 1) / width != ntiles)
+        return pc_fail(ctx, PC_INVALID, "inconsistent subtile geometry");
+    if (stats) memset(stats, 0, sizeof(*stats));
+    auto t0 = std::chrono::steady_clock::now();
+    BatchIO io{counts, geometry, out, out_cap, n_out, stats};
+    int rc = run_device(ctx, f, tuning, us->d + u_off, nu, vs->d + v_off, nv, u128{lo0, lo1}, u128{hi0, hi1}, v_first,
+                        width, ntiles, v_end, io, 0);
+    if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+extern "C" int pc_run_lease(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb, const pc_filters *f,
+                            const pc_tuning *tuning, uint64_t first, uint64_t end, uint64_t width, uint64_t lo0,
+                            uint64_t lo1, uint64_t hi0, uint64_t hi1, uint64_t *counts, uint64_t *geometry,
+                            uint64_t *out, uint64_t out_cap, uint64_t *n_out, pc_stats *stats) {
+    if (!fa || !fb || !f || width == 0 || end <= first) return pc_fail(ctx, PC_INVALID, "invalid lease arguments");
+    if (stats) memset(stats, 0, sizeof(*stats));
+    auto t0 = std::chrono::steady_clock::now();
+    typedef unsigned __int128 w128;
+    w128 lo = (w128)lo1 << 64 | lo0, hi = (w128)hi1 << 64 | hi0;
+    w128 ulo = (lo + (w128)first * f->A) / f->B + 1, uhi = (hi + (w128)(end - 1) * f->A) / f->B + 1;
+    if (uhi >> 64) return pc_fail(ctx, PC_INVALID, "u window exceeds 64 bits");
+    uint64_t ntiles64 = (end - first + width - 1) / width;
+    if (ntiles64 >= (UINT64_C(1) << 31)) return pc_fail(ctx, PC_INVALID, "too many subtiles");
+    int launches = 0;
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
+    uint64_t *d_us = nullptr, *d_vs = nullptr, us_bytes = 0, vs_bytes = 0, nu = 0, nv = 0;
+    const uint64_t cap = (UINT64_C(1) << 32) - 1;
+    int rc = pc_window_into(ctx, fa, (uint64_t)ulo, (uint64_t)uhi, cap, &d_us, &us_bytes, &nu, &launches);
+    if (!rc) rc = pc_window_into(ctx, fb, first, end, cap, &d_vs, &vs_bytes, &nv, &launches);
+    if (!rc) {
+        cudaEventRecord(ctx->ev[5], ctx->stream);
+        BatchIO io{counts, geometry, out, out_cap, n_out, stats};
+        rc = run_device(ctx, f, tuning, d_us ? d_us : (const uint64_t *)nullptr, nu, d_vs, nv, u128{lo0, lo1},
+                        u128{hi0, hi1}, first, width, (uint32_t)ntiles64, end, io, launches);
+        if (stats) stats->window_ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+    }
+    pc_release(ctx, d_us, us_bytes);
+    pc_release(ctx, d_vs, vs_bytes);
+    if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+extern "C" int pc_run_plain(pc_ctx *ctx, const pc_filters *f, const pc_buf *us, uint64_t u_off, uint64_t nu,
+                            const pc_buf *vs, uint64_t v_off, uint64_t nv, uint64_t lo0, uint64_t lo1, uint64_t hi0,
+                            uint64_t hi1, uint64_t *counts, uint64_t *out, uint64_t out_cap, pc_stats *stats) {
+    if (!f || !us || !vs) return pc_fail(ctx, PC_INVALID, "invalid plain arguments");
+    if (u_off > us->n || nu > us->n - u_off || v_off > vs->n || nv > vs->n - v_off)
+        return pc_fail(ctx, PC_INVALID, "focus list slice out of range");
+    if (stats) memset(stats, 0, sizeof(*stats));
+    const uint32_t ng = f->ng;
+    Scratch s(ctx);
+    uint64_t *d_counts, *d_out;
+    int rc = s.get(&d_counts, ng + 3);
+    if (!rc) rc = s.get(&d_out, 2 * std::max<uint64_t>(1, out_cap));
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    PC_CHECK(ctx, cudaMemsetAsync(d_counts, 0, (ng + 3) * 8, st));
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[6], st));
+    if (nu && nv) {
+        PlainArgs a{};
+        a.us = us->d + u_off;
+        a.vs = vs->d + v_off;
+        a.nu = nu;
+        a.nv = nv;
+        a.A = f->A;
+        a.B = f->B;
+        a.lo = u128{lo0, lo1};
+        a.hi = u128{hi0, hi1};
+        a.nres = f->nres;
+        a.ng = ng;
+        a.fc = f->d_fc;
+        a.bits = f->d_bits;
+        a.counts = d_counts;
+        a.out = d_out;
+        a.out_cap = out_cap;
+        uint64_t blocks = std::min<uint64_t>((nv + 7) / 8, (uint64_t)ctx->sm_count * 8);
+        k_plain<<<(unsigned)blocks, 256, 0, st>>>(a);
+        PC_LAUNCHED(ctx, "plain match");
+    }
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[7], st));
+    PC_CHECK(ctx, cudaMemcpyAsync(counts, d_counts, (ng + 3) * 8, cudaMemcpyDeviceToHost, st));
+    PC_CHECK(ctx, cudaStreamSynchronize(st));
+    uint64_t n = counts[ng + 1];
+    if (stats) {
+        stats->kernel_ms = elapsed_ms(ctx->ev[6], ctx->ev[7]);
+        stats->outputs = n;
+        stats->launches = nu && nv ? 1 : 0;
+    }
+    uint64_t copy = std::min(n, out_cap);
+    if (copy) {
+        PC_CHECK(ctx, cudaMemcpyAsync(out, d_out, 2 * copy * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, cudaStreamSynchronize(st));
+    }
+    return PC_OK;
+}

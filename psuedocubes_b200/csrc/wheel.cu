@@ -1,0 +1,492 @@
+// Stage 1: CRT focus-wheel tables and sorted focus windows.
+//
+// A focus of modulus M is the set of y >= 0 whose residue mod every ring modulus q | M lies in
+// the ring's (coefficient-adjusted) allowed set R_q.  Split the rings into S (small moduli) and
+// T (the largest few).  With M1 = prod(S), the sorted wheel W1 = {w in [0, M1): w mod q in R_q
+// for q in S} is built once by a bitset sieve over [0, M1).  Every y = K*M1 + w (w in W1)
+// satisfies the S rings; it is in the focus iff (K*M1 + w) mod q in R_q for the T rings.  For
+// each T ring and each s in [0, q), a bitset row over W1's index space marks the w with
+// (s + w) mod q in R_q; the window for period K is the AND of the rows s = K*M1 mod q.
+//
+// A window [low, high) is therefore walked in (period, wheel index) order, which is ascending
+// value order: a count pass, an exclusive scan and an emit pass produce the sorted values with
+// no sort and no residue set materialised.  Tables are p-independent for p above the largest
+// focus prime.
+#include "common.cuh"
+#include <algorithm>
+#include <chrono>
+#include <numeric>
+
+struct pc_focus {
+    uint64_t M = 0, M1 = 1, count1 = 0, words1 = 0;
+    uint32_t nT = 0;
+    uint32_t tq[PC_MAX_WHEEL_T] = {};
+    uint32_t t_m1mod[PC_MAX_WHEEL_T] = {};
+    uint32_t t_row0[PC_MAX_WHEEL_T] = {};
+    uint32_t total_rows = 0;
+    uint64_t *W1 = nullptr;      // device, sorted wheel
+    uint32_t *rows = nullptr;    // device, total_rows x words1
+    uint64_t W1_bytes = 0, rows_bytes = 0;
+    std::vector<uint64_t> W1_host;
+    uint64_t count_lo = 0, count_hi = 0;
+    double build_ms = 0;
+};
+
+namespace {
+
+constexpr int WT = 256;          // threads per CTA of the window kernels
+constexpr int SIEVE_WORDS = 64;  // sieve words per thread
+constexpr int WIN_WORDS = 32;    // wheel words per window unit
+
+// Periodic bit patterns of the S rings, replicated so any 32-bit window at offset < q is one
+// funnel shift of two consecutive words.
+struct SieveRings {
+    uint32_t n;
+    uint32_t q[16];
+    uint32_t off[16];            // word offset of each ring's pattern in the pattern array
+    uint32_t step[16];           // 32 mod q
+    ModQ mq[16];
+};
+
+__global__ void k_sieve(const SieveRings rings, const uint32_t *__restrict__ patterns, uint64_t M1,
+                        uint64_t nwords, uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
+                        uint64_t *__restrict__ out) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t w0 = t * SIEVE_WORDS;
+    if (w0 >= nwords) return;
+    uint64_t w1 = min(nwords, w0 + SIEVE_WORDS);
+    uint32_t s[16];
+    for (uint32_t r = 0; r < rings.n; ++r) s[r] = mod64(w0 * 32, rings.mq[r]);
+    uint64_t total = 0, pos = offsets ? offsets[t] : 0;
+    for (uint64_t w = w0; w < w1; ++w) {
+        uint32_t bits = 0xffffffffu;
+        for (uint32_t r = 0; r < rings.n; ++r) {
+            const uint32_t *p = patterns + rings.off[r];
+            uint32_t lo = p[s[r] >> 5], hi = p[(s[r] >> 5) + 1];
+            bits &= __funnelshift_r(lo, hi, s[r] & 31);
+            s[r] += rings.step[r];
+            if (s[r] >= rings.q[r]) s[r] -= rings.q[r];
+        }
+        uint64_t base = w * 32;
+        if (base + 32 > M1) bits &= low_bits((uint32_t)(M1 - base));
+        if (offsets) {
+            while (bits) {
+                uint32_t b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                out[pos++] = base + b;
+            }
+        } else {
+            total += __popc(bits);
+        }
+    }
+    if (!offsets) counts[t] = total;
+}
+
+// rows[row0 + s][w] bit l = R[(s + W1[32w + l] mod q) mod q], via the rotation of the pattern
+// RR (R repeated) by m = W1 mod q and a warp transpose.
+__global__ void k_wheel_rows(const uint64_t *__restrict__ W1, uint64_t count1, uint64_t words1,
+                             const uint32_t *__restrict__ pattern, uint32_t q, ModQ mq,
+                             uint32_t *__restrict__ rows) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    if (w >= words1) return;
+    uint64_t j = w * 32 + lane;
+    bool valid = j < count1;
+    uint32_t m = valid ? mod64(W1[j], mq) : 0;
+    for (uint32_t k = 0; k * 32 < q; ++k) {
+        uint32_t st = 32 * k + m;
+        uint32_t col = __funnelshift_r(pattern[st >> 5], pattern[(st >> 5) + 1], st & 31);
+        col = valid ? col : 0u;
+        uint32_t row = transpose32(col, lane);
+        uint32_t s = 32 * k + lane;
+        if (s < q) rows[(uint64_t)s * words1 + w] = row;
+    }
+}
+
+struct WindowPlan {
+    uint64_t K0, K1, j_lo, j_hi;
+    uint64_t wa0, wb0, wa1, wb1;       // word ranges of the first and last period
+    uint64_t units_first, units_mid, units_last, units;
+};
+
+struct WindowArgs {
+    uint64_t M1, count1, words1;
+    uint32_t nT;
+    uint32_t tq[PC_MAX_WHEEL_T];
+    uint32_t t_m1mod[PC_MAX_WHEEL_T];
+    uint32_t t_row0[PC_MAX_WHEEL_T];
+    ModQ tmq[PC_MAX_WHEEL_T];
+    WindowPlan plan;
+};
+
+__device__ __forceinline__ void unit_of(const WindowPlan &p, uint64_t words1, uint64_t u, uint64_t &K,
+                                        uint64_t &wa, uint64_t &wb) {
+    if (u < p.units_first) {
+        K = p.K0;
+        wa = p.wa0 + u * WIN_WORDS;
+        wb = min(p.wb0, wa + WIN_WORDS);
+        return;
+    }
+    u -= p.units_first;
+    uint64_t mid_periods = p.K1 > p.K0 + 1 ? p.K1 - p.K0 - 1 : 0;
+    if (u < mid_periods * p.units_mid) {
+        K = p.K0 + 1 + u / p.units_mid;
+        wa = (u % p.units_mid) * WIN_WORDS;
+        wb = min(words1, wa + WIN_WORDS);
+        return;
+    }
+    u -= mid_periods * p.units_mid;
+    K = p.K1;
+    wa = p.wa1 + u * WIN_WORDS;
+    wb = min(p.wb1, wa + WIN_WORDS);
+}
+
+__global__ void k_window(const WindowArgs a, const uint64_t *__restrict__ W1, const uint32_t *__restrict__ rows,
+                         uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
+                         uint64_t *__restrict__ out) {
+    uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (u >= a.plan.units) return;
+    uint64_t K, wa, wb;
+    unit_of(a.plan, a.words1, u, K, wa, wb);
+    const uint32_t *r[PC_MAX_WHEEL_T];
+    for (uint32_t t = 0; t < a.nT; ++t) {
+        uint32_t s = (uint32_t)(((uint64_t)mod64(K, a.tmq[t]) * a.t_m1mod[t]) % a.tq[t]);
+        r[t] = rows + (uint64_t)(a.t_row0[t] + s) * a.words1;
+    }
+    uint64_t jmin = K == a.plan.K0 ? a.plan.j_lo : 0;
+    uint64_t jmax = K == a.plan.K1 ? a.plan.j_hi : a.count1;
+    uint64_t base = K * a.M1, total = 0, pos = offsets ? offsets[u] : 0;
+    for (uint64_t w = wa; w < wb; ++w) {
+        uint32_t bits = 0xffffffffu;
+        for (uint32_t t = 0; t < a.nT; ++t) bits &= __ldg(r[t] + w);
+        uint64_t j0 = w * 32;
+        if (j0 < jmin) bits &= ~low_bits((uint32_t)(jmin - j0 < 32 ? jmin - j0 : 32));
+        if (j0 + 32 > jmax) bits &= jmax > j0 ? low_bits((uint32_t)(jmax - j0)) : 0u;
+        if (offsets) {
+            while (bits) {
+                uint32_t b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                out[pos++] = base + __ldg(W1 + j0 + b);
+            }
+        } else {
+            total += __popc(bits);
+        }
+    }
+    if (!offsets) counts[u] = total;
+}
+
+// 128-bit product of 64-bit counts, host side.
+void mul_acc(uint64_t &lo, uint64_t &hi, uint64_t f) {
+    unsigned __int128 v = ((unsigned __int128)hi << 64 | lo) * f;
+    lo = (uint64_t)v;
+    hi = (uint64_t)(v >> 64);
+}
+
+uint64_t gcd64(uint64_t a, uint64_t b) {
+    while (b) {
+        uint64_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+}  // namespace
+
+extern "C" int pc_focus_create(pc_ctx *ctx, uint64_t M, uint32_t nrings, const uint32_t *q, const uint32_t *counts,
+                               const uint32_t *residues, uint64_t table_budget, pc_focus **out) {
+    *out = nullptr;
+    if (M == 0 || M >= (UINT64_C(1) << 63) || nrings > 16) return pc_fail(ctx, PC_INVALID, "invalid focus modulus");
+    auto t_start = std::chrono::steady_clock::now();
+    if (!table_budget) table_budget = UINT64_C(256) << 20;
+    struct Ring {
+        uint32_t q, n;
+        std::vector<uint32_t> res;
+    };
+    std::vector<Ring> rings;
+    uint64_t prodq = 1, off = 0;
+    for (uint32_t k = 0; k < nrings; ++k) {
+        Ring r{q[k], counts[k], std::vector<uint32_t>(residues + off, residues + off + counts[k])};
+        off += counts[k];
+        if (r.q < 2 || r.q > 65535 || r.n == 0 || r.n > r.q) return pc_fail(ctx, PC_INVALID, "invalid ring");
+        for (uint32_t a : r.res)
+            if (a >= r.q) return pc_fail(ctx, PC_INVALID, "ring residue out of range");
+        if (M % r.q || gcd64(M / r.q, r.q) != 1) return pc_fail(ctx, PC_INVALID, "ring moduli must be coprime factors of M");
+        prodq *= r.q;
+        rings.push_back(std::move(r));
+    }
+    if (prodq != M) return pc_fail(ctx, PC_INVALID, "ring moduli do not multiply to M");
+    std::sort(rings.begin(), rings.end(), [](const Ring &a, const Ring &b) { return a.q < b.q; });
+
+    pc_focus *f = new pc_focus();
+    f->M = M;
+    f->count_lo = 1;
+    for (auto &r : rings) mul_acc(f->count_lo, f->count_hi, r.n);
+    // Choose the T rings: the fewest largest rings whose removal makes the sieve over M1 and
+    // the tables fit; among the feasible, the smallest table budget use wins ties.
+    uint32_t chosen = UINT32_MAX;
+    for (uint32_t nT = 0; nT <= std::min<uint32_t>(PC_MAX_WHEEL_T, nrings); ++nT) {
+        uint64_t M1 = M, count1_lo = f->count_lo, count1_hi = f->count_hi, rowsum = 0;
+        for (uint32_t k = nrings - nT; k < nrings; ++k) {
+            M1 /= rings[k].q;
+            rowsum += rings[k].q;
+            unsigned __int128 c = ((unsigned __int128)count1_hi << 64 | count1_lo) / rings[k].n;
+            count1_lo = (uint64_t)c;
+            count1_hi = (uint64_t)(c >> 64);
+        }
+        if (count1_hi || M1 > (UINT64_C(1) << 36)) continue;
+        uint64_t words1 = (count1_lo + 31) / 32;
+        uint64_t bytes = count1_lo * 8 + rowsum * words1 * 4;
+        if (bytes <= table_budget) {
+            chosen = nT;
+            break;
+        }
+    }
+    if (chosen == UINT32_MAX) {
+        delete f;
+        return pc_fail(ctx, PC_INVALID, "focus wheel does not fit the table budget");
+    }
+    f->nT = chosen;
+    uint32_t nS = nrings - chosen;
+    f->M1 = 1;
+    for (uint32_t k = 0; k < nS; ++k) f->M1 *= rings[k].q;
+
+    // --- W1: sieve over [0, M1) with the S rings
+    SieveRings sr{};
+    sr.n = nS;
+    std::vector<uint32_t> pat;
+    for (uint32_t k = 0; k < nS; ++k) {
+        const Ring &r = rings[k];
+        sr.q[k] = r.q;
+        sr.off[k] = (uint32_t)pat.size();
+        sr.step[k] = 32 % r.q;
+        sr.mq[k] = make_modq(r.q);
+        uint32_t nbits = r.q + 64;
+        std::vector<uint32_t> words((nbits + 31) / 32 + 1, 0);
+        std::vector<char> ok(r.q, 0);
+        for (uint32_t a : r.res) ok[a] = 1;
+        for (uint32_t b = 0; b < nbits; ++b)
+            if (ok[b % r.q]) words[b / 32] |= 1u << (b % 32);
+        pat.insert(pat.end(), words.begin(), words.end());
+    }
+    Scratch s(ctx);
+    uint32_t *d_pat;
+    int rc = s.get(&d_pat, pat.size() + 1);
+    if (rc) {
+        delete f;
+        return rc;
+    }
+    if (!pat.empty()) cudaMemcpyAsync(d_pat, pat.data(), pat.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+    uint64_t nwords = (f->M1 + 31) / 32;
+    uint64_t nthreads = (nwords + SIEVE_WORDS - 1) / SIEVE_WORDS;
+    uint64_t *d_cnt, *d_off, *d_total;
+    rc = s.get(&d_cnt, nthreads);
+    if (!rc) rc = s.get(&d_off, nthreads);
+    if (!rc) rc = s.get(&d_total, 1);
+    if (rc) {
+        delete f;
+        return rc;
+    }
+    unsigned grid = (unsigned)((nthreads + WT - 1) / WT);
+    k_sieve<<<grid, WT, 0, ctx->stream>>>(sr, d_pat, f->M1, nwords, d_cnt, nullptr, nullptr);
+    rc = pc_exclusive_scan_u64(ctx, d_cnt, d_off, nthreads, d_total);
+    uint64_t total = 0;
+    if (!rc && cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream) == cudaSuccess &&
+        cudaStreamSynchronize(ctx->stream) == cudaSuccess) {
+    } else if (!rc) {
+        rc = pc_cuda_fail(ctx, cudaGetLastError(), "wheel count");
+    }
+    if (rc) {
+        delete f;
+        return rc;
+    }
+    uint64_t expect_lo = f->count_lo, expect_hi = f->count_hi;
+    for (uint32_t k = nS; k < nrings; ++k) {
+        unsigned __int128 c = ((unsigned __int128)expect_hi << 64 | expect_lo) / rings[k].n;
+        expect_lo = (uint64_t)c;
+        expect_hi = (uint64_t)(c >> 64);
+    }
+    if (total != expect_lo || expect_hi) {
+        delete f;
+        return pc_fail(ctx, PC_ARITHMETIC, "wheel size disagrees with the ring counts");
+    }
+    f->count1 = total;
+    f->words1 = (total + 31) / 32;
+    f->W1_bytes = std::max<uint64_t>(16, total * 8);
+    rc = pc_alloc(ctx, (void **)&f->W1, f->W1_bytes);
+    if (rc) {
+        delete f;
+        return rc;
+    }
+    k_sieve<<<grid, WT, 0, ctx->stream>>>(sr, d_pat, f->M1, nwords, nullptr, d_off, f->W1);
+    PC_LAUNCHED(ctx, "wheel sieve");
+
+    // --- rows of the T rings
+    f->total_rows = 0;
+    for (uint32_t t = 0; t < chosen; ++t) {
+        f->tq[t] = rings[nS + t].q;
+        f->t_m1mod[t] = (uint32_t)(f->M1 % f->tq[t]);
+        f->t_row0[t] = f->total_rows;
+        f->total_rows += f->tq[t];
+    }
+    f->rows_bytes = std::max<uint64_t>(16, (uint64_t)f->total_rows * f->words1 * 4);
+    rc = pc_alloc(ctx, (void **)&f->rows, f->rows_bytes);
+    if (rc) {
+        pc_release(ctx, f->W1, f->W1_bytes);
+        delete f;
+        return rc;
+    }
+    for (uint32_t t = 0; t < chosen; ++t) {
+        const Ring &r = rings[nS + t];
+        uint32_t nbits = 2 * r.q + 64;
+        std::vector<uint32_t> words((nbits + 31) / 32 + 1, 0);
+        std::vector<char> ok(r.q, 0);
+        for (uint32_t a : r.res) ok[a] = 1;
+        for (uint32_t b = 0; b < nbits; ++b)
+            if (ok[b % r.q]) words[b / 32] |= 1u << (b % 32);
+        uint32_t *d_rp;
+        rc = s.get(&d_rp, words.size());
+        if (rc) break;
+        cudaMemcpyAsync(d_rp, words.data(), words.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+        uint64_t threads = f->words1 * 32;
+        k_wheel_rows<<<(unsigned)((threads + WT - 1) / WT), WT, 0, ctx->stream>>>(
+            f->W1, f->count1, f->words1, d_rp, r.q, make_modq(r.q), f->rows + (uint64_t)f->t_row0[t] * f->words1);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            rc = pc_cuda_fail(ctx, e, "wheel rows");
+            break;
+        }
+    }
+    if (!rc) {
+        f->W1_host.resize(f->count1);
+        cudaError_t e = cudaMemcpyAsync(f->W1_host.data(), f->W1, f->count1 * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = pc_cuda_fail(ctx, e, "wheel download");
+    }
+    if (rc) {
+        pc_release(ctx, f->W1, f->W1_bytes);
+        pc_release(ctx, f->rows, f->rows_bytes);
+        delete f;
+        return rc;
+    }
+    f->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    *out = f;
+    return PC_OK;
+}
+
+extern "C" int pc_focus_free(pc_ctx *ctx, pc_focus *f) {
+    if (!f) return PC_OK;
+    pc_release(ctx, f->W1, f->W1_bytes);
+    pc_release(ctx, f->rows, f->rows_bytes);
+    delete f;
+    return PC_OK;
+}
+
+extern "C" int pc_focus_info(const pc_focus *f, uint64_t *info) {
+    info[0] = f->M;
+    info[1] = f->M1;
+    info[2] = f->count1;
+    info[3] = f->nT;
+    info[4] = f->W1_bytes + f->rows_bytes;
+    info[5] = f->count_lo;
+    info[6] = f->count_hi;
+    info[7] = (uint64_t)f->build_ms;
+    return PC_OK;
+}
+
+// Plan and run one window; out is allocated by the call (out_bytes returned for release).
+// total_host receives the count.  Exported to the batch/lease code through this declaration.
+int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, uint64_t cap,
+                   uint64_t **out, uint64_t *out_bytes, uint64_t *total_host, int *launches) {
+    *out = nullptr;
+    *out_bytes = 0;
+    *total_host = 0;
+    if (high < low) return pc_fail(ctx, PC_INVALID, "invalid bounded focus window");
+    if (high == low) return PC_OK;
+    if ((high - 1) / f->M - low / f->M + 1 > 4096) return pc_fail(ctx, PC_OVERFLOW, "focus window exceeds bounded period count");
+    WindowArgs a{};
+    a.M1 = f->M1;
+    a.count1 = f->count1;
+    a.words1 = f->words1;
+    a.nT = f->nT;
+    for (uint32_t t = 0; t < f->nT; ++t) {
+        a.tq[t] = f->tq[t];
+        a.t_m1mod[t] = f->t_m1mod[t];
+        a.t_row0[t] = f->t_row0[t];
+        a.tmq[t] = make_modq(f->tq[t]);
+    }
+    WindowPlan &p = a.plan;
+    p.K0 = low / f->M1;
+    p.K1 = (high - 1) / f->M1;
+    const std::vector<uint64_t> &W = f->W1_host;
+    p.j_lo = std::lower_bound(W.begin(), W.end(), low - p.K0 * f->M1) - W.begin();
+    p.j_hi = std::lower_bound(W.begin(), W.end(), high - p.K1 * f->M1) - W.begin();
+    if (p.K0 == p.K1) {
+        p.wa0 = p.j_lo / 32;
+        p.wb0 = std::max(p.wa0, (p.j_hi + 31) / 32);
+        p.wa1 = p.wb1 = 0;
+    } else {
+        p.wa0 = p.j_lo / 32;
+        p.wb0 = f->words1;
+        p.wa1 = 0;
+        p.wb1 = (p.j_hi + 31) / 32;
+    }
+    p.units_first = (p.wb0 - p.wa0 + WIN_WORDS - 1) / WIN_WORDS;
+    p.units_mid = (f->words1 + WIN_WORDS - 1) / WIN_WORDS;
+    p.units_last = p.K1 > p.K0 ? (p.wb1 - p.wa1 + WIN_WORDS - 1) / WIN_WORDS : 0;
+    uint64_t mid_periods = p.K1 > p.K0 + 1 ? p.K1 - p.K0 - 1 : 0;
+    p.units = p.units_first + mid_periods * p.units_mid + p.units_last;
+    if (p.units == 0) return PC_OK;
+    Scratch s(ctx);
+    uint64_t *d_cnt, *d_off, *d_total;
+    int rc = s.get(&d_cnt, p.units);
+    if (!rc) rc = s.get(&d_off, p.units);
+    if (!rc) rc = s.get(&d_total, 1);
+    if (rc) return rc;
+    unsigned grid = (unsigned)((p.units + WT - 1) / WT);
+    k_window<<<grid, WT, 0, ctx->stream>>>(a, f->W1, f->rows, d_cnt, nullptr, nullptr);
+    PC_LAUNCHED(ctx, "window count");
+    rc = pc_exclusive_scan_u64(ctx, d_cnt, d_off, p.units, d_total);
+    if (rc) return rc;
+    uint64_t total = 0;
+    PC_CHECK(ctx, cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+    *total_host = total;
+    if (total > cap) return pc_fail(ctx, PC_OVERFLOW, "focus buffer overflow; tile invalid");
+    uint64_t bytes = std::max<uint64_t>(16, total * 8);
+    rc = pc_alloc(ctx, (void **)out, bytes);
+    if (rc) return rc;
+    *out_bytes = bytes;
+    k_window<<<grid, WT, 0, ctx->stream>>>(a, f->W1, f->rows, nullptr, d_off, *out);
+    PC_LAUNCHED(ctx, "window emit");
+    if (launches) *launches += 2 + 3;
+    return PC_OK;
+}
+
+extern "C" int pc_focus_window(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, uint64_t cap,
+                               pc_buf **out, uint64_t *count) {
+    *out = nullptr;
+    *count = 0;
+    uint64_t *d = nullptr, bytes = 0, total = 0;
+    int rc = pc_window_into(ctx, f, low, high, cap, &d, &bytes, &total, nullptr);
+    *count = total;
+    if (rc) {
+        pc_release(ctx, d, bytes);
+        return rc;
+    }
+    pc_buf *b = new pc_buf();
+    b->d = d;
+    b->n = total;
+    b->bytes = bytes;
+    if (!d) {
+        rc = pc_alloc(ctx, (void **)&b->d, 16);
+        if (rc) {
+            delete b;
+            return rc;
+        }
+        b->bytes = 16;
+    }
+    PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = b;
+    return PC_OK;
+}

@@ -1,0 +1,145 @@
+"""Host-side logic of the product package against the reference's fixtures (no GPU)."""
+from __future__ import annotations
+
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden
+from psuedocubes_b200 import _native as N
+from psuedocubes_b200.accounting import digest, encoded
+from psuedocubes_b200.batch_experiment import split_outputs, tile_ranges
+from psuedocubes_b200.focus import A619, B619, Config, Tile, targeted_coordinates
+from psuedocubes_b200.gpu import launch_plan
+from psuedocubes_b200.multi import validate_result
+from psuedocubes_b200.optimized import BATCH_WIDTH, Accumulator
+from psuedocubes_b200.predicate import icbrt, is_perfect_cube, local3, qualifies3
+from psuedocubes_b200.tables import allowed, definition, packed, sieve_primes
+from psuedocubes_b200.verify import verify
+
+
+def test_library_exports_every_declared_symbol():
+    header = (ROOT / 'include' / 'pcube.h').read_text()
+    declared = set(re.findall(r'^\s*(?:int|const char \*)\s*(pc_\w+)\s*\(', header, re.M))
+    assert declared == set(N.SYMBOLS)
+    lib = N.lib()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert lib.pc_version() == 1
+
+
+def test_tables_and_predicate():
+    t = golden('tables.json')
+    assert definition(619)['sha256'] == t['sha256_619']
+    assert definition(67)['sha256'] == t['sha256_67']
+    assert list(allowed(31)) == t['allowed_31'] and list(allowed(9)) == t['allowed_9']
+    cubic = [q for q in sieve_primes(619) if q % 3 == 1]
+    assert (len(sieve_primes(619)), len(cubic), sum(cubic)) == (114, 54, 15744)
+    assert sum(4 * len(packed(q)) for q in cubic) == t['packed_cubic_bytes_619'] == 2076
+    known = golden('known.json')
+    assert icbrt(3 * 10**27) == known['icbrt_3e27']
+    assert local3(int(known['cases'][0]['n']), 619) == known['n613_local3_619']
+    for case in known['cases']:
+        n, p = int(case['n']), case['p']
+        assert local3(n, p) == case['local3'] and is_perfect_cube(n) == case['cube']
+        assert verify(n, p) == case['verify']
+    for bad in (2, 3, 5, 9, 15, 25, -7):
+        with pytest.raises(ValueError):
+            local3(1, bad)
+    assert local3(1, 619) and not qualifies3(1, 619)
+
+
+def test_geometry_matches_reference(p619):
+    g = golden('geometry.json')
+    assert p619.manifest() == g['manifest_619']
+    assert p619.filter_order() == g['residual_order_619']
+    af, bf = p619.focuses()
+    assert [[q, list(r)] for q, r in af.rings] == g['focus_rings_619']['A']
+    assert [[q, list(r)] for q, r in bf.rings] == g['focus_rings_619']['B']
+    for n, u, v, lo, hi in g['canonical']:
+        assert p619.canonical(int(n)) == (int(u), int(v))
+        assert p619.u_interval(int(v)) == (int(lo), int(hi))
+    for case in g['tile_ranges']:
+        rows = tile_ranges(p619, int(case['first']), int(case['end']), case['width'])
+        assert [[str(x) for x in row] for row in rows] == case['rows']
+    with pytest.raises(ValueError):
+        tile_ranges(p619, 0, 65, 1)
+    with pytest.raises(ValueError):
+        tile_ranges(p619, 0, 1, 0)
+
+
+def test_small_manifests_match_reference():
+    for case in golden('small_sets.json'):
+        c = Config(case['p'], case['lo'], case['hi'], case['A'], case['B'])
+        assert c.manifest() == case['manifest']
+        assert c.filter_order() == case['residual_order']
+    case = golden('p67_prefix.json')
+    assert Config(67, 1, 10**13, case['A'], case['B']).manifest() == case['manifest']
+
+
+def test_targeted_coordinates_match_reference():
+    for case in golden('known.json')['cases']:
+        n, p = int(case['n']), case['p']
+        c = Config(p, max(0, n - 100), min(3 * 10**27, n + 100), A619, B619)
+        us, vs = targeted_coordinates(c, n)
+        assert [str(x) for x in us] == case['us'] and [str(x) for x in vs] == case['vs']
+        assert [str(x) for x in c.canonical(n)] == case['canonical']
+
+
+def test_config_rejections():
+    with pytest.raises(ValueError):
+        Config(7, 0, 100000, 14, 9 * 13)
+    with pytest.raises(ValueError):
+        Config(7, 0, 100000, 3 * 7, 3)
+    with pytest.raises(ValueError):
+        Tile(5, 5).validate(Config(619, 10**27, 3 * 10**27, A619, B619))
+
+
+def test_encoded_is_canonical():
+    assert encoded({'b': 1, 'a': [1 << 53, 2]}) == b'{"a":["9007199254740992",2],"b":1}\n'
+    assert digest([]) == '37517e5f3dc66819f61f5a7bb8ace1921282415f10551d2defa5c3eb0985b570'
+
+
+def test_launch_plan_partitions_every_candidate():
+    for nu in (0, 1, 31, 32, 33, 63, 255, 256, 257, 6001):
+        for nv in (0, 1, 7, 8, 9, 86, 289, 962):
+            for target in (1, 2, 4):
+                blocks, stripes = launch_plan(nu, nv, 84, 'warp', target)
+                assert bool(blocks) == bool(nu and nv)
+                if blocks:
+                    assert blocks * 8 >= nv * stripes and blocks * 8 - nv * stripes < 8
+    assert launch_plan(6001, 86, 84, 'serial') == (1, 1)
+    for layout, target in (('unknown', 2), ('warp', 0), ('warp', True), ('warp', 3)):
+        with pytest.raises(ValueError):
+            launch_plan(10, 10, 84, layout, target)
+
+
+def test_split_outputs_groups_and_sorts():
+    x1, x2, x3 = 10**27 + 7, 10**27 + 3, 2 * 10**27 + 11
+    recs = np.array([[x & (2**64 - 1), (x >> 64) | (t << 32)] for x, t in ((x1, 1), (x2, 1), (x3, 0))],
+                    dtype=np.uint64)
+    assert split_outputs(recs, 3) == [[x3], [x2, x1], []]
+
+
+def test_accumulator_rejects_gaps_and_bad_receipts():
+    acc = Accumulator(0, 2 * BATCH_WIDTH)
+    with pytest.raises(ValueError):
+        acc.add(BATCH_WIDTH, 2 * BATCH_WIDTH, {})
+    with pytest.raises(ValueError):
+        validate_result(0, 10, dict(status='FAIL'))
+    with pytest.raises(ValueError):
+        validate_result(0, 10, dict(status='PASS', host_verified=True,
+                                    subtile_scopes=[dict(first='0', end='5')], valid_focused_candidates=0,
+                                    genuine_cubes=0))
+    with pytest.raises(ValueError):
+        Accumulator(0, 0)
+
+
+def test_status_codes_map_to_reference_exceptions():
+    for code, exc in ((N.PC_OVERFLOW, OverflowError), (N.PC_INVALID, ValueError), (N.PC_ARITHMETIC, ArithmeticError),
+                      (N.PC_TIMEOUT, TimeoutError), (N.PC_NOMEM, MemoryError), (N.PC_CUDA, RuntimeError)):
+        with pytest.raises(exc):
+            N.raise_for(code, None, 'x')
+    N.raise_for(N.PC_OK)
