@@ -42,7 +42,8 @@ constexpr int PATW = 136;            // pattern words per bitset filter (q <= 20
 constexpr int TMAX_DEFAULT = 64;     // subtile counter slots per CTA
 
 struct __align__(16) VRec {
-    uint32_t left, right, tile, pad;
+    uint32_t left, right;            // exact u interval as indices into the sorted u list
+    uint64_t v;
     uint16_t row[8];                 // row index (row0 + v mod q) of each bitset filter
 };
 
@@ -72,6 +73,8 @@ struct MatchArgs {
     const uint64_t *item_prefix;     // nblocks + 1
     uint64_t nblocks;
     const uint64_t *vchunk;          // device scalar
+    uint64_t v_first, width;         // subtile of v = (v - v_first) / width
+    uint32_t stage;                  // v records per shared-memory staging chunk
 };
 
 // first j with us[j] * B > key
@@ -118,49 +121,66 @@ struct PrepArgs {
     unsigned long long *bad;
 };
 
-// Per v row: exact u interval as list indices (batch_experiment.py:209-215), subtile, bitset
-// row indices, and focused-position count of the subtile (popcount of the range masks there).
+// Per v row: exact u interval as list indices (batch_experiment.py:209-215), bitset row
+// indices, and the focused-position count of its subtile.  A thread owns PREP_RUN consecutive v
+// rows: one binary search per bound for the first, then the monotone bounds advance linearly
+// (about N_u/N_v < 1 step per row).
+constexpr int PREP_RUN = 16;
+
+__device__ __forceinline__ uint64_t advance_le(const uint64_t *__restrict__ us, uint64_t n, uint64_t B, u128 key,
+                                               uint64_t from) {
+    for (int step = 0; step < 16; ++step) {
+        if (from >= n || less128(key, mul_wide(__ldg(us + from), B))) return from;
+        ++from;
+    }
+    return from + count_le(us + from, n - from, B, key);   // long gap: binary search the rest
+}
+
 __global__ void k_vprep(const PrepArgs a) {
-    uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    const uint32_t lane = threadIdx.x & 31;
-    uint64_t tile = UINT64_MAX, pop0 = 0;
-    if (j < a.nv) {
-        uint64_t v = a.vs[j];
-        u128 shift = mul_wide(v, a.A);
-        uint64_t left = count_le(a.us, a.nu, a.B, add128(shift, a.lo));
-        uint64_t right = count_le(a.us, a.nu, a.B, add128(shift, a.hi));
-        if (right < left) right = left;
-        if (v < a.v_first) {
-            atomicAdd(a.bad, 1ull);
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t j0 = t * PREP_RUN;
+    if (j0 >= a.nv) return;
+    const uint64_t j1 = umin64(a.nv, j0 + PREP_RUN);
+    uint64_t left = 0, right = 0, tile = UINT64_MAX, t_lo = 1, t_hi = 0, pop = 0;
+    for (uint64_t j = j0; j < j1; ++j) {
+        const uint64_t v = a.vs[j];
+        const u128 shift = mul_wide(v, a.A);
+        const u128 klo = add128(shift, a.lo), khi = add128(shift, a.hi);
+        if (j == j0) {
+            left = count_le(a.us, a.nu, a.B, klo);
+            right = umax64(left, count_le(a.us, a.nu, a.B, khi));
         } else {
-            tile = tile_of(v, a.v_first, a.width);
-            if (tile >= a.ntiles) {
+            left = advance_le(a.us, a.nu, a.B, klo, left);
+            right = advance_le(a.us, a.nu, a.B, khi, umax64(left, right));
+        }
+        if (v < t_lo || v >= t_hi) {
+            if (tile != UINT64_MAX && pop)
+                atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3)], (unsigned long long)pop);
+            pop = 0;
+            if (v < a.v_first) {
                 atomicAdd(a.bad, 1ull);
-                tile = UINT64_MAX;
+                tile = UINT64_MAX, t_lo = 1, t_hi = 0;
+            } else {
+                tile = tile_of(v, a.v_first, a.width);
+                t_lo = a.v_first + tile * a.width;
+                t_hi = t_lo + a.width;
+                if (tile >= a.ntiles) {
+                    atomicAdd(a.bad, 1ull);
+                    tile = UINT64_MAX, t_lo = 1, t_hi = 0;
+                }
             }
         }
         VRec r;
         r.left = (uint32_t)left;
         r.right = (uint32_t)right;
-        r.tile = tile == UINT64_MAX ? 0u : (uint32_t)tile;
-        r.pad = 0;
+        r.v = v;
 #pragma unroll
         for (int f = 0; f < PC_MAX_BITSET; ++f)
             r.row[f] = f < (int)a.nb ? (uint16_t)(a.row0[f] + mod64(v, a.mq[f])) : (uint16_t)0;
         a.rec[j] = r;
-        pop0 = right - left;
+        pop += right - left;
     }
-    // warp-aggregated subtile sums (consecutive v rows mostly share a subtile)
-    uint64_t t0 = __shfl_sync(0xffffffffu, tile, 0);
-    bool same = __all_sync(0xffffffffu, tile == t0 || tile == UINT64_MAX);
-    if (same) {
-        uint64_t s = pop0;
-#pragma unroll
-        for (int d = 16; d; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
-        if (lane == 0 && t0 != UINT64_MAX && s) atomicAdd((unsigned long long *)&a.counts[t0 * (a.ng + 3)], (unsigned long long)s);
-    } else if (tile != UINT64_MAX && pop0) {
-        atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3)], (unsigned long long)pop0);
-    }
+    if (tile != UINT64_MAX && pop) atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3)], (unsigned long long)pop);
 }
 
 // Per subtile: u count and v count of its envelope (searchsorted bounds of
@@ -285,6 +305,27 @@ __device__ __forceinline__ bool later_filters(const MatchArgs &a, u128 x, uint32
     return true;
 }
 
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.
+struct MatchSmem {
+    uint32_t rows, us, recs, pat, cnt, total;
+    __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t stage, uint32_t tmax,
+                                  uint32_t ng) {
+        rows = 0;
+        us = rows + total_rows * (K / 4) * 16;
+        recs = us + K * 32 * 8;
+        pat = recs + 2 * stage * (uint32_t)sizeof(VRec);
+        cnt = pat + nb * PATW * 4;
+        total = cnt + tmax * (ng + 2) * 4;
+    }
+};
+
 template <int NB, int K>
 __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
     using G = Geo<K>;
@@ -292,14 +333,18 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
     constexpr int LPV = K / WPL;          // lanes per v row
     constexpr int VPW = 32 / LPV;         // v rows per warp step
     extern __shared__ uint4 smem[];
-    uint4 *rows = smem;
-    uint64_t *us_s = (uint64_t *)(rows + (size_t)a.total_rows * G::U);
-    uint32_t *pat_s = (uint32_t *)(us_s + G::UB);
-    uint32_t *cnt_s = pat_s + NB * PATW;                  // tmax x (ng+2): groups 1..ng, outputs
+    const MatchSmem L(a.total_rows, K, NB, a.stage, a.tmax, a.ng);
+    char *base = (char *)smem;
+    uint4 *rows = (uint4 *)(base + L.rows);
+    uint64_t *us_s = (uint64_t *)(base + L.us);
+    VRec *recs = (VRec *)(base + L.recs);
+    uint32_t *pat_s = (uint32_t *)(base + L.pat);
+    uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ng+2): groups 1..ng, outputs
     const uint32_t stride = a.ng + 2;
 
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint32_t gsel = lane / LPV, sub = lane % LPV;
+    const uint32_t stage = a.stage;
 
     for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = a.pat[i];
 
@@ -318,6 +363,13 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
     }
     const bool c2_live = NB == 8 || (NB > 4 && NB == (int)a.nres);
 
+    auto issue = [&](uint64_t from, uint64_t count, uint32_t buf) {
+        const char *src = (const char *)(a.rec + from);
+        char *dst = (char *)(recs + (size_t)buf * stage);
+        for (uint32_t k = threadIdx.x; k < count * 2; k += blockDim.x) cp_async16(dst + 16 * k, src + 16 * k);
+        cp_async_commit();
+    };
+
     for (uint64_t it = i0; it < i1; ++it) {
         while (a.item_prefix[bsearch + 1] <= it) ++bsearch;  // items are visited in order
         const uint64_t b = bsearch;
@@ -325,7 +377,9 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
         const uint64_t va = range.x + (it - a.item_prefix[b]) * vch;
         const uint64_t vb = umin64(range.y, va + vch);
         const uint64_t block_u0 = b * G::UB;
-        __syncthreads();                                  // previous item finished with smem
+        __syncthreads();                                  // previous item finished with shared memory
+        const uint64_t nch = (vb - va + stage - 1) / stage;
+        issue(va, umin64(stage, vb - va), 0);             // first chunk of records overlaps the row build
         if (b != cur) {
             for (uint32_t k = threadIdx.x; k < G::UB; k += blockDim.x)
                 us_s[k] = block_u0 + k < a.nu ? a.us[block_u0 + k] : 0;
@@ -334,109 +388,114 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
             cur = b;
         }
         for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) cnt_s[k] = 0;
-        __syncthreads();
-        const uint32_t tile_base = a.rec[va].tile;
+        const uint64_t tile_base = tile_of(a.rec[va].v, a.v_first, a.width);
 
-        uint32_t c1 = 0, c2 = 0, ctile = UINT32_MAX;
+        uint32_t c1 = 0, c2 = 0;
+        uint64_t ctile = UINT64_MAX, t_lo = 1, t_hi = 0;  // current subtile and its v range
         auto flush = [&]() {
-            if (ctile == UINT32_MAX || (c1 == 0 && c2 == 0)) return;
-            uint32_t slot = ctile - tile_base;
+            if (ctile == UINT64_MAX || (c1 == 0 && c2 == 0)) return;
+            uint64_t slot = ctile - tile_base;
             if (slot < a.tmax) {
                 if (c1) atomicAdd(cnt_s + slot * stride + 1, c1);
                 if (c2) atomicAdd(cnt_s + slot * stride + 2, c2);
             } else {
-                if (c1) atomicAdd((unsigned long long *)&a.counts[(uint64_t)ctile * (a.ng + 3) + 1], (unsigned long long)c1);
-                if (c2) atomicAdd((unsigned long long *)&a.counts[(uint64_t)ctile * (a.ng + 3) + 2], (unsigned long long)c2);
+                if (c1) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 1], (unsigned long long)c1);
+                if (c2) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 2], (unsigned long long)c2);
             }
             c1 = c2 = 0;
         };
 
-        for (uint64_t v0 = va + (uint64_t)warp * VPW; v0 < vb; v0 += (uint64_t)nwarps * VPW) {
-            const uint64_t vi = v0 + gsel;
-            const bool active = vi < vb;
-            VRec r;
-            if (active) r = a.rec[vi];
-            else {
-                r.left = r.right = 0;
-                r.tile = ctile;
-#pragma unroll
-                for (int f = 0; f < 8; ++f) r.row[f] = a.row0[0];
-            }
-            int64_t s = (int64_t)r.left - (int64_t)block_u0, e = (int64_t)r.right - (int64_t)block_u0;
-            s = imax64(s, 0);
-            e = imin64(e, G::UB);
-            if (!active || e < s) e = s;
-            const int32_t lb = sub * WPL * 32;
-            int32_t ls = (int32_t)imin64(imax64(s - lb, 0), WPL * 32);
-            int32_t le = (int32_t)imin64(imax64(e - lb, 0), WPL * 32);
+        for (uint64_t ch = 0; ch < nch; ++ch) {
+            const uint64_t cstart = va + ch * stage;
+            const uint32_t cn = (uint32_t)umin64(stage, vb - cstart);
+            if (ch + 1 < nch) issue(cstart + stage, umin64(stage, vb - cstart - stage), (uint32_t)((ch + 1) & 1));
+            else cp_async_commit();
+            cp_async_wait1();
+            __syncthreads();
+            const VRec *cb = recs + (size_t)(ch & 1) * stage;
 
-            uint4 acc = rows[G::unit(r.row[0], sub)];
-            uint4 acc4;
+            for (uint32_t v0 = warp * VPW; v0 < cn; v0 += nwarps * VPW) {
+                const uint32_t vloc = v0 + gsel;
+                const bool active = vloc < cn;
+                const VRec r = cb[active ? vloc : 0];
+                int64_t s = (int64_t)r.left - (int64_t)block_u0, e = (int64_t)r.right - (int64_t)block_u0;
+                s = imax64(s, 0);
+                e = imin64(e, G::UB);
+                if (!active || e < s) e = s;
+                const int32_t lb = sub * WPL * 32;
+                int32_t ls = (int32_t)imin64(imax64(s - lb, 0), WPL * 32);
+                int32_t le = (int32_t)imin64(imax64(e - lb, 0), WPL * 32);
+
+                uint4 acc = rows[G::unit(r.row[0], sub)];
+                uint4 acc4;
 #pragma unroll
-            for (int f = 1; f < NB; ++f) {
-                if (f == 4) acc4 = acc;
-                uint4 x = rows[G::unit(r.row[f], sub)];
-                acc.x &= x.x;
-                acc.y &= x.y;
-                acc.z &= x.z;
-                acc.w &= x.w;
-            }
-            if (NB <= 4) acc4 = acc;
-            uint32_t w4[4] = {acc4.x, acc4.y, acc4.z, acc4.w};
-            uint32_t wn[4] = {acc.x, acc.y, acc.z, acc.w};
-            if (ls > 0 || le < WPL * 32) {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    int32_t a0 = min(max(ls - 32 * k, 0), 32), a1 = min(max(le - 32 * k, 0), 32);
-                    uint32_t m = low_bits((uint32_t)a1) & ~low_bits((uint32_t)a0);
-                    w4[k] &= m;
-                    wn[k] &= m;
+                for (int f = 1; f < NB; ++f) {
+                    if (f == 4) acc4 = acc;
+                    uint4 x = rows[G::unit(r.row[f], sub)];
+                    acc.x &= x.x;
+                    acc.y &= x.y;
+                    acc.z &= x.z;
+                    acc.w &= x.w;
                 }
-            }
-            if (active && r.tile != ctile) {
-                flush();
-                ctile = r.tile;
-            }
-            c1 += __popc(w4[0]) + __popc(w4[1]) + __popc(w4[2]) + __popc(w4[3]);
-            if (c2_live) c2 += __popc(wn[0]) + __popc(wn[1]) + __popc(wn[2]) + __popc(wn[3]);
-
-            bool more = (wn[0] | wn[1] | wn[2] | wn[3]) != 0;
-            if (__any_sync(0xffffffffu, more)) {
-                const uint64_t v = active ? a.vs[vi] : 0;
-                const u128 shift = mul_wide(v, a.A);
-                const uint32_t slot = r.tile - tile_base;
-                uint32_t *cs = slot < a.tmax ? cnt_s + slot * stride : nullptr;
-                while (__any_sync(0xffffffffu, more)) {
-                    if (more) {
-                        uint32_t local = 0;
+                if (NB <= 4) acc4 = acc;
+                uint32_t w4[4] = {acc4.x, acc4.y, acc4.z, acc4.w};
+                uint32_t wn[4] = {acc.x, acc.y, acc.z, acc.w};
+                if (ls > 0 || le < WPL * 32) {
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            if (wn[k]) {
-                                uint32_t bit = __ffs(wn[k]) - 1;
-                                wn[k] &= wn[k] - 1;
-                                local = lb + 32 * k + bit;
-                                break;
+                    for (int k = 0; k < 4; ++k) {
+                        int32_t a0 = min(max(ls - 32 * k, 0), 32), a1 = min(max(le - 32 * k, 0), 32);
+                        uint32_t m = low_bits((uint32_t)a1) & ~low_bits((uint32_t)a0);
+                        w4[k] &= m;
+                        wn[k] &= m;
+                    }
+                }
+                if (active && (r.v < t_lo || r.v >= t_hi)) {
+                    flush();
+                    ctile = tile_of(r.v, a.v_first, a.width);
+                    t_lo = a.v_first + ctile * a.width;
+                    t_hi = t_lo + a.width;
+                }
+                c1 += __popc(w4[0]) + __popc(w4[1]) + __popc(w4[2]) + __popc(w4[3]);
+                if (c2_live) c2 += __popc(wn[0]) + __popc(wn[1]) + __popc(wn[2]) + __popc(wn[3]);
+
+                bool more = (wn[0] | wn[1] | wn[2] | wn[3]) != 0;
+                if (__any_sync(0xffffffffu, more)) {
+                    const u128 shift = mul_wide(r.v, a.A);
+                    const uint64_t slot = ctile - tile_base;
+                    uint32_t *cs = more && slot < a.tmax ? cnt_s + slot * stride : nullptr;
+                    while (__any_sync(0xffffffffu, more)) {
+                        if (more) {
+                            uint32_t local = 0;
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                if (wn[k]) {
+                                    uint32_t bit = __ffs(wn[k]) - 1;
+                                    wn[k] &= wn[k] - 1;
+                                    local = lb + 32 * k + bit;
+                                    break;
+                                }
                             }
-                        }
-                        more = (wn[0] | wn[1] | wn[2] | wn[3]) != 0;
-                        const u128 pos = mul_wide(us_s[local], a.B);
-                        if (less128(pos, shift)) {
-                            atomicAdd((unsigned long long *)&a.counts[(uint64_t)r.tile * (a.ng + 3) + a.ng + 2], 1ull);
-                        } else {
-                            const u128 x = sub128(pos, shift);
-                            if (later_filters(a, x, NB, cs, r.tile)) {
-                                if (cs) atomicAdd(cs + a.ng + 1, 1u);
-                                else atomicAdd((unsigned long long *)&a.counts[(uint64_t)r.tile * (a.ng + 3) + a.ng + 1], 1ull);
-                                unsigned long long o = atomicAdd(a.n_out, 1ull);
-                                if (o < a.out_cap) {
-                                    a.out[2 * o] = x.lo;
-                                    a.out[2 * o + 1] = x.hi | ((uint64_t)r.tile << 32);
+                            more = (wn[0] | wn[1] | wn[2] | wn[3]) != 0;
+                            const u128 pos = mul_wide(us_s[local], a.B);
+                            if (less128(pos, shift)) {
+                                atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + a.ng + 2], 1ull);
+                            } else {
+                                const u128 x = sub128(pos, shift);
+                                if (later_filters(a, x, NB, cs, ctile)) {
+                                    if (cs) atomicAdd(cs + a.ng + 1, 1u);
+                                    else atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + a.ng + 1], 1ull);
+                                    unsigned long long o = atomicAdd(a.n_out, 1ull);
+                                    if (o < a.out_cap) {
+                                        a.out[2 * o] = x.lo;
+                                        a.out[2 * o + 1] = x.hi | (ctile << 32);
+                                    }
                                 }
                             }
                         }
                     }
                 }
             }
+            __syncthreads();                              // buffer (ch & 1) is refilled at chunk ch + 2
         }
         flush();
         __syncthreads();
@@ -444,7 +503,7 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
             uint32_t c = cnt_s[k];
             if (c) {
                 uint32_t slot = k / stride, g = k % stride;
-                uint64_t tile = (uint64_t)tile_base + slot;
+                uint64_t tile = tile_base + slot;
                 if (tile < a.ntiles)
                     atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], (unsigned long long)c);
             }
@@ -641,7 +700,7 @@ extern "C" int pc_filters_free(pc_ctx *ctx, pc_filters *f) {
 namespace {
 
 struct Tuned {
-    uint32_t nb, K, threads;
+    uint32_t nb, K, threads, stage;
     uint64_t v_chunk;
 };
 
@@ -659,14 +718,16 @@ Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
     if (optin <= 0) optin = 227 * 1024;
     for (;;) {
-        size_t rows = (size_t)f->rows_sum[r.nb] * (r.K / 4) * 16;
-        size_t fixed = rows + (size_t)r.K * 32 * 8 + (size_t)r.nb * PATW * 4;
-        size_t per_slot = (size_t)(f->ng + 2) * 4;
-        if (fixed + per_slot * 4 <= (size_t)optin) {
-            uint32_t tmax = (uint32_t)std::min<size_t>(TMAX_DEFAULT, ((size_t)optin - fixed) / per_slot);
-            *tmax_out = tmax;
-            *smem_out = fixed + per_slot * tmax;
-            return r;
+        for (uint32_t stage = 512; stage >= 64; stage /= 2) {
+            for (uint32_t tmax = TMAX_DEFAULT; tmax >= 4; tmax /= 2) {
+                MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, stage, tmax, f->ng);
+                if (L.total <= (uint32_t)optin) {
+                    r.stage = stage;
+                    *tmax_out = tmax;
+                    *smem_out = L.total;
+                    return r;
+                }
+            }
         }
         if (r.K > 16) r.K /= 2;
         else if (r.nb > nb_min) r.nb--;
@@ -740,7 +801,8 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
     pa.counts = d_counts;
     pa.bad = d_bad;
     if (nv) {
-        k_vprep<<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(pa);
+        uint64_t runs = (nv + PREP_RUN - 1) / PREP_RUN;
+        k_vprep<<<(unsigned)((runs + 127) / 128), 128, 0, st>>>(pa);
         PC_LAUNCHED(ctx, "vprep");
         ++launches;
     }
@@ -799,6 +861,9 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
         ma.item_prefix = d_prefix;
         ma.nblocks = nblocks;
         ma.vchunk = d_vchunk;
+        ma.v_first = v_first;
+        ma.width = width;
+        ma.stage = tn.stage;
         PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
         if (tn.K == 16) rc = launch_match_k<16>(ctx, ma, smem, tn.threads, grid);
         else if (tn.K == 32) rc = launch_match_k<32>(ctx, ma, smem, tn.threads, grid);
