@@ -41,12 +41,13 @@ def seeded_first_batch() -> int:
     return random.Random(619003).randrange(0, BATCHES_TOTAL - 1 - LEASE_BATCHES + 1)
 
 
-def lease_bounds(index: int) -> tuple[int, int]:
+def lease_bounds(index: int, batches: int = LEASE_BATCHES) -> tuple[int, int]:
     from psuedocubes_b200.focus import B619
-    from psuedocubes_b200.optimized import BATCH_WIDTH, LEASE_WIDTH
-    first = (seeded_first_batch() * BATCH_WIDTH + index * LEASE_WIDTH) % (B619 - LEASE_WIDTH)
+    from psuedocubes_b200.optimized import BATCH_WIDTH
+    width = batches * BATCH_WIDTH
+    first = (seeded_first_batch() * BATCH_WIDTH + index * width) % (B619 - width)
     first -= first % BATCH_WIDTH
-    return first, first + LEASE_WIDTH
+    return first, first + width
 
 
 class ClockSampler:
@@ -170,7 +171,7 @@ def run_ours(args) -> None:
     af, bf = (GPUFocus(runtime, f) for f in config.focuses())
     matcher = MaskedMatcher(runtime, config)
     width = PROFILE['tile_width']
-    nt = (LEASE_BATCHES * 64)
+    nt = args.lease_batches * 64
     ng = len(matcher.filter_groups)
     counts = np.zeros(nt * (ng + 3), dtype=np.uint64)
     geometry = np.zeros(2 * nt, dtype=np.uint64)
@@ -182,7 +183,7 @@ def run_ours(args) -> None:
     c = config
 
     def step(index: int) -> tuple[int, dict]:
-        first, end = lease_bounds(index * world + rank)
+        first, end = lease_bounds(index * world + rank, args.lease_batches)
         runtime.call(lib.pc_run_lease(ctx, af.handle, bf.handle, matcher.filters.handle, ctypes.byref(matcher.tuning),
                                       first, end, width, c.lo & MASK, c.lo >> 64, c.hi & MASK, c.hi >> 64, counts,
                                       geometry, records, cap, ctypes.byref(n_out), ctypes.byref(stats)))
@@ -208,14 +209,14 @@ def run_ours(args) -> None:
     total_positions = positions * world   # every rank runs the same number of equal-size leases
     # end to end through the public API: compute_lease with host assembly, verification, transcript
     barrier(dist)
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = args.e2e_steps
     t0 = time.perf_counter()
     e2e_positions = 0
     for k in range(e2e_steps):
-        first, end = lease_bounds((args.warmup + args.steps + k) * world + rank)
+        first, end = lease_bounds((args.warmup + args.steps + k) * world + rank, args.lease_batches)
         result = compute_lease(matcher, af, bf, first, end)
         e2e_positions += result['valid_focused_candidates']
-    e2e_seconds = max_over_ranks(dist, time.perf_counter() - t0, local)
+    e2e_seconds = max_over_ranks(dist, time.perf_counter() - t0, local) if e2e_steps else 0.0
     d2h = counts.nbytes + geometry.nbytes + 16 + 16 * (outputs // max(1, args.steps))
     if rank == 0:
         clock = clocks.summary()
@@ -227,14 +228,14 @@ def run_ours(args) -> None:
                     scaling='weak', vs_baseline=None, dtype='u64', data='synthetic',
                     config=dict(workload='p=619 production lease: 256 batches x 64 subtiles x 1e8 canonical v, '
                                          'Config(619, 10^27, 3*10^27, A619, B619)',
-                                first_batch=seeded_first_batch(), lease_batches=LEASE_BATCHES, parallelism=f'replicas{world}',
+                                first_batch=seeded_first_batch(), lease_batches=args.lease_batches, parallelism=f'replicas{world}',
                                 l2='inputs larger than L2 (resident wheel tables 208 MB, per-lease lists and bounds ~0.7 GB)'),
                     roofline=dict(bound='int_alu', achieved=achieved, peak=peak, unit='Tlaneop/s',
                                   frac=achieved / peak if achieved else None, traffic=None,
                                   kernel='k_match (fused bitset + 128-bit filters)',
                                   ops_per_position=OPS_PER_POSITION,
                                   peak_basis=f'{runtime.sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz'),
-                    e2e=dict(value=e2e_positions * world / e2e_seconds, unit=UNIT, h2d_bytes_per_step=0,
+                    e2e=dict(value=e2e_positions * world / e2e_seconds if e2e_seconds else None, unit=UNIT, h2d_bytes_per_step=0,
                              d2h_bytes_per_step=int(d2h), api='psuedocubes_b200.optimized.compute_lease'),
                     gpu_launches=launches, clocks=clock,
                     kernel_ms_per_step=kernel_ms / args.steps)
@@ -255,6 +256,9 @@ def main() -> None:
     parser.add_argument('--warmup', type=int, default=3)
     parser.add_argument('--impl', choices=('ours', 'reference'), default='ours')
     parser.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    parser.add_argument('--lease-batches', type=int, default=LEASE_BATCHES,
+                        help='batches per step (256 = a full lease; smaller only for profiling)')
+    parser.add_argument('--e2e-steps', type=int, default=2)
     args = parser.parse_args()
     if args.impl == 'reference':
         run_reference(args)
