@@ -23,6 +23,16 @@ struct FiltConst {
     uint32_t pad;
 };
 
+// Compact filter constants passed inside the kernel parameters (constant bank): fast remainder
+// constant, modulus, bitmap offset and 2^(16k) mod q for k = 1..5 (x < 2^96).
+struct FiltC {
+    uint64_t c;
+    uint32_t q, tab_off;
+    uint16_t r16[5];
+    uint16_t pad[3];
+};
+constexpr int FC_INLINE = 128;
+
 struct pc_filters {
     uint64_t A = 0, B = 0;
     uint32_t nres = 0, ng = 0;
@@ -34,6 +44,7 @@ struct pc_filters {
     uint32_t nbmax = 0;              // filters usable as bitset rows
     uint32_t ainvb[PC_MAX_BITSET] = {};
     uint32_t rows_sum[PC_MAX_BITSET + 1] = {};   // prefix sums of q over the first filters
+    std::vector<FiltC> fcs;
 };
 
 namespace {
@@ -75,6 +86,7 @@ struct MatchArgs {
     const uint64_t *vchunk;          // device scalar
     uint64_t v_first, width;         // subtile of v = (v - v_first) / width
     uint32_t stage;                  // v records per shared-memory staging chunk
+    FiltC fcs[FC_INLINE];            // residual filters in order (the first nres are used)
 };
 
 // first j with us[j] * B > key
@@ -288,23 +300,6 @@ __device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, const u
     }
 }
 
-// Arithmetic filters idx = first..nres-1 on a survivor; group counters into shared slots.
-// Returns true if x passes every filter.
-__device__ __forceinline__ bool later_filters(const MatchArgs &a, u128 x, uint32_t first, uint32_t *cnt_slot,
-                                              uint64_t tile) {
-    for (uint32_t idx = first; idx < a.nres; ++idx) {
-        const FiltConst fc = a.fc[idx];
-        uint32_t m = mod128(x, fc.m);
-        if (!((__ldg(a.bits + fc.tab_off + (m >> 5)) >> (m & 31)) & 1u)) return false;
-        if ((idx & 3) == 3 || idx + 1 == a.nres) {
-            uint32_t g = idx / 4 + 1;
-            if (cnt_slot) atomicAdd(cnt_slot + g, 1u);
-            else atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], 1ull);
-        }
-    }
-    return true;
-}
-
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gmem) : "memory");
@@ -312,19 +307,29 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
+constexpr int QCAP = 64;   // survivor ring per warp (pending < 64 by construction)
+
 // Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.
 struct MatchSmem {
-    uint32_t rows, us, recs, pat, cnt, total;
+    uint32_t rows, us, recs, queue, pat, cnt, total;
     __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t stage, uint32_t tmax,
-                                  uint32_t ng) {
+                                  uint32_t ng, uint32_t warps) {
         rows = 0;
         us = rows + total_rows * (K / 4) * 16;
         recs = us + K * 32 * 8;
-        pat = recs + 2 * stage * (uint32_t)sizeof(VRec);
+        queue = recs + 2 * stage * (uint32_t)sizeof(VRec);
+        pat = queue + warps * QCAP * 8;
         cnt = pat + nb * PATW * 4;
         total = cnt + tmax * (ng + 2) * 4;
     }
 };
+
+// x mod q for x < 2^96 from its six 16-bit limbs h (h[0] + sum h[k] (2^16k mod q), then one
+// fast remainder; every partial sum stays below 2^32 because q < 2^13).
+__device__ __forceinline__ uint32_t mod_limbs(const uint32_t h[6], const FiltC &f) {
+    uint32_t t = h[0] + h[1] * f.r16[0] + h[2] * f.r16[1] + h[3] * f.r16[2] + h[4] * f.r16[3] + h[5] * f.r16[4];
+    return fastmod32(t, f.c, f.q);
+}
 
 template <int NB, int K>
 __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
@@ -333,18 +338,19 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
     constexpr int LPV = K / WPL;          // lanes per v row
     constexpr int VPW = 32 / LPV;         // v rows per warp step
     extern __shared__ uint4 smem[];
-    const MatchSmem L(a.total_rows, K, NB, a.stage, a.tmax, a.ng);
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const MatchSmem L(a.total_rows, K, NB, a.stage, a.tmax, a.ng, nwarps);
     char *base = (char *)smem;
     uint4 *rows = (uint4 *)(base + L.rows);
     uint64_t *us_s = (uint64_t *)(base + L.us);
     VRec *recs = (VRec *)(base + L.recs);
+    uint64_t *queue = (uint64_t *)(base + L.queue) + warp * QCAP;
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
     uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ng+2): groups 1..ng, outputs
     const uint32_t stride = a.ng + 2;
-
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint32_t gsel = lane / LPV, sub = lane % LPV;
     const uint32_t stage = a.stage;
+    const uint32_t lanes_below = (1u << lane) - 1u;
 
     for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = a.pat[i];
 
@@ -376,7 +382,7 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
         const uint2 range = a.bv[b];
         const uint64_t va = range.x + (it - a.item_prefix[b]) * vch;
         const uint64_t vb = umin64(range.y, va + vch);
-        const uint64_t block_u0 = b * G::UB;
+        const uint32_t block_u0 = (uint32_t)(b * G::UB);
         __syncthreads();                                  // previous item finished with shared memory
         const uint64_t nch = (vb - va + stage - 1) / stage;
         issue(va, umin64(stage, vb - va), 0);             // first chunk of records overlaps the row build
@@ -391,18 +397,83 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
         const uint64_t tile_base = tile_of(a.rec[va].v, a.v_first, a.width);
 
         uint32_t c1 = 0, c2 = 0;
-        uint64_t ctile = UINT64_MAX, t_lo = 1, t_hi = 0;  // current subtile and its v range
+        uint64_t ctile = UINT64_MAX, t_lo = 1, t_hi = 0;  // this lane's subtile and its v range
+        uint32_t qhead = 0, qtail = 0;                    // warp-uniform ring positions
+
+        // group-1/2 populations of every lane, reduced over lanes of the same subtile
         auto flush = [&]() {
-            if (ctile == UINT64_MAX || (c1 == 0 && c2 == 0)) return;
-            uint64_t slot = ctile - tile_base;
-            if (slot < a.tmax) {
-                if (c1) atomicAdd(cnt_s + slot * stride + 1, c1);
-                if (c2) atomicAdd(cnt_s + slot * stride + 2, c2);
-            } else {
-                if (c1) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 1], (unsigned long long)c1);
-                if (c2) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 2], (unsigned long long)c2);
+            const uint64_t key = (c1 | c2) ? ctile : UINT64_MAX - 1 - lane;
+            const uint32_t same = __match_any_sync(0xffffffffu, key);
+            const uint32_t s1 = __reduce_add_sync(same, c1), s2 = __reduce_add_sync(same, c2);
+            if (key == ctile && lane == (uint32_t)(__ffs(same) - 1)) {
+                const uint64_t slot = ctile - tile_base;
+                if (slot < a.tmax) {
+                    if (s1) atomicAdd(cnt_s + slot * stride + 1, s1);
+                    if (s2) atomicAdd(cnt_s + slot * stride + 2, s2);
+                } else {
+                    if (s1) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 1], (unsigned long long)s1);
+                    if (s2) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 2], (unsigned long long)s2);
+                }
             }
             c1 = c2 = 0;
+        };
+
+        // Exact later filters on up to 32 queued survivors, one per lane.
+        auto drain = [&](uint32_t n, const VRec *cb) {
+            __syncwarp();
+            const bool mine = lane < n;
+            const uint64_t e = mine ? queue[(qhead + lane) & (QCAP - 1)] : 0;
+            __syncwarp();
+            qhead += n;
+            bool pass = false;
+            u128 x{0, 0};
+            uint64_t tile = 0;
+            if (mine) {
+                const uint32_t uidx = (uint32_t)(e & 0xffff), vloc = (uint32_t)((e >> 16) & 0xffff);
+                const uint64_t slot = e >> 32;
+                tile = tile_base + slot;
+                const u128 pos = mul_wide(us_s[uidx], a.B), shift = mul_wide(cb[vloc].v, a.A);
+                uint32_t *cs = slot < a.tmax ? cnt_s + slot * stride : nullptr;
+                if (less128(pos, shift)) {
+                    atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 2], 1ull);
+                } else {
+                    x = sub128(pos, shift);
+                    uint32_t h[6] = {(uint32_t)x.lo & 0xffffu, (uint32_t)(x.lo >> 16) & 0xffffu,
+                                     (uint32_t)(x.lo >> 32) & 0xffffu, (uint32_t)(x.lo >> 48),
+                                     (uint32_t)x.hi & 0xffffu, (uint32_t)(x.hi >> 16) & 0xffffu};
+                    pass = true;
+                    for (uint32_t idx = NB; idx < a.nres; ++idx) {
+                        const FiltC f = a.fcs[idx];
+                        const uint32_t m = mod_limbs(h, f);
+                        if (!((__ldg(a.bits + f.tab_off + (m >> 5)) >> (m & 31)) & 1u)) {
+                            pass = false;
+                            break;
+                        }
+                        if ((idx & 3) == 3 || idx + 1 == a.nres) {
+                            const uint32_t g = idx / 4 + 1;
+                            if (cs) atomicAdd(cs + g, 1u);
+                            else atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], 1ull);
+                        }
+                    }
+                    if (pass) {
+                        if (cs) atomicAdd(cs + a.ng + 1, 1u);
+                        else atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 1], 1ull);
+                    }
+                }
+            }
+            const uint32_t won = __ballot_sync(0xffffffffu, pass);
+            if (won) {
+                unsigned long long base_slot = 0;
+                if (lane == (uint32_t)(__ffs(won) - 1)) base_slot = atomicAdd(a.n_out, (unsigned long long)__popc(won));
+                base_slot = __shfl_sync(0xffffffffu, base_slot, __ffs(won) - 1);
+                if (pass) {
+                    const unsigned long long o = base_slot + __popc(won & lanes_below);
+                    if (o < a.out_cap) {
+                        a.out[2 * o] = x.lo;
+                        a.out[2 * o + 1] = x.hi | (tile << 32);
+                    }
+                }
+            }
         };
 
         for (uint64_t ch = 0; ch < nch; ++ch) {
@@ -418,83 +489,69 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
                 const uint32_t vloc = v0 + gsel;
                 const bool active = vloc < cn;
                 const VRec r = cb[active ? vloc : 0];
-                int64_t s = (int64_t)r.left - (int64_t)block_u0, e = (int64_t)r.right - (int64_t)block_u0;
-                s = imax64(s, 0);
-                e = imin64(e, G::UB);
-                if (!active || e < s) e = s;
                 const int32_t lb = sub * WPL * 32;
-                int32_t ls = (int32_t)imin64(imax64(s - lb, 0), WPL * 32);
-                int32_t le = (int32_t)imin64(imax64(e - lb, 0), WPL * 32);
-
+                int32_t ls = 0, le = 0;
+                if (active) {
+                    const int32_t s = max((int32_t)(r.left - block_u0), 0);   // indices < 2^31
+                    const int32_t e = min((int32_t)(r.right - block_u0), (int32_t)G::UB);
+                    ls = min(max(s - lb, 0), WPL * 32);
+                    le = min(max(e - lb, 0), WPL * 32);
+                    le = max(le, ls);
+                }
                 uint4 acc = rows[G::unit(r.row[0], sub)];
                 uint4 acc4;
 #pragma unroll
                 for (int f = 1; f < NB; ++f) {
                     if (f == 4) acc4 = acc;
-                    uint4 x = rows[G::unit(r.row[f], sub)];
-                    acc.x &= x.x;
-                    acc.y &= x.y;
-                    acc.z &= x.z;
-                    acc.w &= x.w;
+                    const uint4 w = rows[G::unit(r.row[f], sub)];
+                    acc.x &= w.x;
+                    acc.y &= w.y;
+                    acc.z &= w.z;
+                    acc.w &= w.w;
                 }
                 if (NB <= 4) acc4 = acc;
-                uint32_t w4[4] = {acc4.x, acc4.y, acc4.z, acc4.w};
-                uint32_t wn[4] = {acc.x, acc.y, acc.z, acc.w};
                 if (ls > 0 || le < WPL * 32) {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        int32_t a0 = min(max(ls - 32 * k, 0), 32), a1 = min(max(le - 32 * k, 0), 32);
-                        uint32_t m = low_bits((uint32_t)a1) & ~low_bits((uint32_t)a0);
-                        w4[k] &= m;
-                        wn[k] &= m;
-                    }
+                    const uint32_t m0 = low_bits((uint32_t)min(max(le, 0), 32)) & ~low_bits((uint32_t)min(max(ls, 0), 32));
+                    const uint32_t m1 = low_bits((uint32_t)min(max(le - 32, 0), 32)) & ~low_bits((uint32_t)min(max(ls - 32, 0), 32));
+                    const uint32_t m2 = low_bits((uint32_t)min(max(le - 64, 0), 32)) & ~low_bits((uint32_t)min(max(ls - 64, 0), 32));
+                    const uint32_t m3 = low_bits((uint32_t)min(max(le - 96, 0), 32)) & ~low_bits((uint32_t)min(max(ls - 96, 0), 32));
+                    acc.x &= m0, acc.y &= m1, acc.z &= m2, acc.w &= m3;
+                    acc4.x &= m0, acc4.y &= m1, acc4.z &= m2, acc4.w &= m3;
                 }
-                if (active && (r.v < t_lo || r.v >= t_hi)) {
+                const bool moved = active && (r.v < t_lo || r.v >= t_hi);
+                if (__any_sync(0xffffffffu, moved)) {
                     flush();
-                    ctile = tile_of(r.v, a.v_first, a.width);
-                    t_lo = a.v_first + ctile * a.width;
-                    t_hi = t_lo + a.width;
-                }
-                c1 += __popc(w4[0]) + __popc(w4[1]) + __popc(w4[2]) + __popc(w4[3]);
-                if (c2_live) c2 += __popc(wn[0]) + __popc(wn[1]) + __popc(wn[2]) + __popc(wn[3]);
-
-                bool more = (wn[0] | wn[1] | wn[2] | wn[3]) != 0;
-                if (__any_sync(0xffffffffu, more)) {
-                    const u128 shift = mul_wide(r.v, a.A);
-                    const uint64_t slot = ctile - tile_base;
-                    uint32_t *cs = more && slot < a.tmax ? cnt_s + slot * stride : nullptr;
-                    while (__any_sync(0xffffffffu, more)) {
-                        if (more) {
-                            uint32_t local = 0;
-#pragma unroll
-                            for (int k = 0; k < 4; ++k) {
-                                if (wn[k]) {
-                                    uint32_t bit = __ffs(wn[k]) - 1;
-                                    wn[k] &= wn[k] - 1;
-                                    local = lb + 32 * k + bit;
-                                    break;
-                                }
-                            }
-                            more = (wn[0] | wn[1] | wn[2] | wn[3]) != 0;
-                            const u128 pos = mul_wide(us_s[local], a.B);
-                            if (less128(pos, shift)) {
-                                atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + a.ng + 2], 1ull);
-                            } else {
-                                const u128 x = sub128(pos, shift);
-                                if (later_filters(a, x, NB, cs, ctile)) {
-                                    if (cs) atomicAdd(cs + a.ng + 1, 1u);
-                                    else atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + a.ng + 1], 1ull);
-                                    unsigned long long o = atomicAdd(a.n_out, 1ull);
-                                    if (o < a.out_cap) {
-                                        a.out[2 * o] = x.lo;
-                                        a.out[2 * o + 1] = x.hi | (ctile << 32);
-                                    }
-                                }
-                            }
-                        }
+                    if (moved) {
+                        ctile = tile_of(r.v, a.v_first, a.width);
+                        t_lo = a.v_first + ctile * a.width;
+                        t_hi = t_lo + a.width;
                     }
+                }
+                c1 += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
+                if (c2_live) c2 += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
+
+                uint64_t sl = (uint64_t)acc.y << 32 | acc.x, sh = (uint64_t)acc.w << 32 | acc.z;
+                const uint32_t slot = (uint32_t)(ctile - tile_base);
+                while (__any_sync(0xffffffffu, (sl | sh) != 0)) {
+                    const bool has = (sl | sh) != 0;
+                    const uint32_t bal = __ballot_sync(0xffffffffu, has);
+                    if (has) {
+                        uint32_t bit;
+                        if (sl) {
+                            bit = __ffsll(sl) - 1;
+                            sl &= sl - 1;
+                        } else {
+                            bit = 64 + __ffsll(sh) - 1;
+                            sh &= sh - 1;
+                        }
+                        const uint32_t pos = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
+                        queue[pos] = (uint64_t)(lb + bit) | ((uint64_t)vloc << 16) | ((uint64_t)slot << 32);
+                    }
+                    qtail += __popc(bal);
+                    if (qtail - qhead >= 32) drain(32, cb);
                 }
             }
+            if (qtail != qhead) drain(qtail - qhead, cb);  // records of this chunk are about to be replaced
             __syncthreads();                              // buffer (ch & 1) is refilled at chunk ch + 2
         }
         flush();
@@ -636,6 +693,12 @@ extern "C" int pc_filters_create(pc_ctx *ctx, uint64_t A, uint64_t B, const uint
         }
         fc[i].m = make_modq(q);
         fc[i].tab_off = (uint32_t)bits.size();
+        FiltC c{};
+        c.c = fc[i].m.c;
+        c.q = q;
+        c.tab_off = fc[i].tab_off;
+        for (int k = 0; k < 5; ++k) c.r16[k] = (uint16_t)fc[i].m.r16[k];
+        f->fcs.push_back(c);
         std::vector<uint32_t> w((q + 31) / 32, 0);
         for (uint32_t r = 0; r < q; ++r)
             if (allowed[off + r]) w[r / 32] |= 1u << (r % 32);
@@ -720,7 +783,7 @@ Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_
     for (;;) {
         for (uint32_t stage = 512; stage >= 64; stage /= 2) {
             for (uint32_t tmax = TMAX_DEFAULT; tmax >= 4; tmax /= 2) {
-                MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, stage, tmax, f->ng);
+                MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, stage, tmax, f->ng, r.threads / 32);
                 if (L.total <= (uint32_t)optin) {
                     r.stage = stage;
                     *tmax_out = tmax;
@@ -748,7 +811,9 @@ struct BatchIO {
 int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const uint64_t *d_us, uint64_t nu,
                const uint64_t *d_vs, uint64_t nv, u128 lo, u128 hi, uint64_t v_first, uint64_t width,
                uint32_t ntiles, uint64_t v_end, const BatchIO &io, int launches0) {
-    if (nu >= (UINT64_C(1) << 32) || nv >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "focus list too long");
+    if (nu >= (UINT64_C(1) << 31) || nv >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "focus list too long");
+    if (hi.hi >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "interval bound must be below 2^96");
+    if (f->nres > (uint32_t)FC_INLINE) return pc_fail(ctx, PC_INVALID, "more residual filters than the fused kernel holds");
     const uint32_t ng = f->ng, stride = ng + 3;
     size_t smem = 0;
     uint32_t tmax = 0;
@@ -821,7 +886,7 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
         if (!rc) rc = s.get(&d_tmp, nblocks + 1);
         if (!rc) rc = pc_exclusive_scan_u64(ctx, d_pieces, d_tmp, nblocks, d_tmp + nblocks);
         if (rc) return rc;
-        k_chunk<<<1, 1, 0, st>>>(d_tmp + nblocks, tn.v_chunk, (uint64_t)grid * 4, d_vchunk);
+        k_chunk<<<1, 1, 0, st>>>(d_tmp + nblocks, tn.v_chunk, (uint64_t)grid * 32, d_vchunk);
         PC_LAUNCHED(ctx, "chunk");
         k_item_counts<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_pieces, nblocks, d_vchunk, d_items);
         PC_LAUNCHED(ctx, "item counts");
@@ -864,6 +929,7 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
         ma.v_first = v_first;
         ma.width = width;
         ma.stage = tn.stage;
+        for (uint32_t i = 0; i < f->nres && i < (uint32_t)FC_INLINE; ++i) ma.fcs[i] = f->fcs[i];
         PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
         if (tn.K == 16) rc = launch_match_k<16>(ctx, ma, smem, tn.threads, grid);
         else if (tn.K == 32) rc = launch_match_k<32>(ctx, ma, smem, tn.threads, grid);
