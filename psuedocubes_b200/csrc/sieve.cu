@@ -80,12 +80,11 @@ struct MatchArgs {
     uint64_t out_cap;
     unsigned long long *n_out;
     uint32_t ntiles;
-    const uint2 *bv;                 // per u block: v index range
+    const uint4 *bv;                 // per u block: v rows meeting it, v rows covering it
     const uint64_t *item_prefix;     // nblocks + 1
     uint64_t nblocks;
     const uint64_t *vchunk;          // device scalar
     uint64_t v_first, width;         // subtile of v = (v - v_first) / width
-    uint32_t stage;                  // v records per shared-memory staging chunk
     FiltC fcs[FC_INLINE];            // residual filters in order (the first nres are used)
 };
 
@@ -211,27 +210,38 @@ __global__ void k_geometry(const uint64_t *__restrict__ us, uint64_t nu, const u
     geometry[2 * s + 1] = vb - va;
 }
 
-// Per u block of UB entries: [va, vb) of v rows whose [left, right) meets the block.
+// Per u block of UB entries: [va, vb) of v rows whose [left, right) meets the block, and the
+// sub-range [f0, f1) of rows covering the whole block (left <= start and right >= stop); left and
+// right are monotone in the row index, so all four are binary searches.
+__device__ __forceinline__ uint64_t first_right_ge(const VRec *__restrict__ rec, uint64_t lo, uint64_t hi, uint64_t x) {
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        if (rec[mid].right >= x) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint64_t first_left_ge(const VRec *__restrict__ rec, uint64_t lo, uint64_t hi, uint64_t x) {
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        if (rec[mid].left >= x) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
 __global__ void k_blocks(const VRec *__restrict__ rec, uint64_t nv, uint64_t nu, uint32_t UB, uint64_t nblocks,
-                         uint2 *__restrict__ bv, uint64_t *__restrict__ pieces) {
+                         uint4 *__restrict__ bv, uint64_t *__restrict__ pieces) {
     uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (b >= nblocks) return;
-    uint64_t start = b * UB, stop = umin64(nu, start + UB);
-    uint64_t lo = 0, hi = nv;                       // first j with right > start
-    while (lo < hi) {
-        uint64_t mid = lo + (hi - lo) / 2;
-        if (rec[mid].right > start) hi = mid;
-        else lo = mid + 1;
-    }
-    uint64_t va = lo;
-    lo = va, hi = nv;                               // first j with left >= stop
-    while (lo < hi) {
-        uint64_t mid = lo + (hi - lo) / 2;
-        if (rec[mid].left >= stop) hi = mid;
-        else lo = mid + 1;
-    }
-    uint64_t vb = lo;
-    bv[b] = make_uint2((uint32_t)va, (uint32_t)vb);
+    const uint64_t start = b * UB, stop = umin64(nu, start + UB);
+    const uint64_t va = first_right_ge(rec, 0, nv, start + 1);
+    const uint64_t vb = first_left_ge(rec, va, nv, stop);
+    uint64_t f0 = umax64(va, first_right_ge(rec, va, vb, stop));
+    uint64_t f1 = umin64(vb, first_left_ge(rec, va, vb, start + 1));
+    if (f1 < f0) f1 = f0;
+    bv[b] = make_uint4((uint32_t)va, (uint32_t)vb, (uint32_t)f0, (uint32_t)f1);
     pieces[b] = vb > va ? vb - va : 0;
 }
 
@@ -258,10 +268,7 @@ template <int K>
 struct Geo {
     static constexpr int U = K / 4;                      // 16-byte units per row
     static constexpr int UB = K * 32;                    // u entries per block
-    static constexpr int SWS = U == 4 ? 1 : 0;           // swizzle shift
-    __device__ static __forceinline__ uint32_t unit(uint32_t row, uint32_t c) {
-        return row * U + (c ^ ((row >> SWS) & (U - 1)));
-    }
+    __device__ static __forceinline__ uint32_t unit(uint32_t row, uint32_t c) { return row * U + c; }
 };
 
 template <int NB, int K>
@@ -300,25 +307,23 @@ __device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, const u
     }
 }
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
 constexpr int QCAP = 64;   // survivor ring per warp (pending < 64 by construction)
+
+struct QEntry {
+    uint64_t v;
+    uint32_t uidx;             // u index within the block
+    uint32_t slot;             // subtile - first subtile of the item
+};
 
 // Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.
 struct MatchSmem {
-    uint32_t rows, us, recs, queue, pat, cnt, total;
-    __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t stage, uint32_t tmax,
-                                  uint32_t ng, uint32_t warps) {
+    uint32_t rows, us, queue, pat, cnt, total;
+    __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t tmax, uint32_t ng,
+                                  uint32_t warps) {
         rows = 0;
         us = rows + total_rows * (K / 4) * 16;
-        recs = us + K * 32 * 8;
-        queue = recs + 2 * stage * (uint32_t)sizeof(VRec);
-        pat = queue + warps * QCAP * 8;
+        queue = us + K * 32 * 8;
+        pat = queue + warps * QCAP * (uint32_t)sizeof(QEntry);
         cnt = pat + nb * PATW * 4;
         total = cnt + tmax * (ng + 2) * 4;
     }
@@ -331,25 +336,27 @@ __device__ __forceinline__ uint32_t mod_limbs(const uint32_t h[6], const FiltC &
     return fastmod32(t, f.c, f.q);
 }
 
+__device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bits [lo, hi) of one 32-bit word
+    return low_bits((uint32_t)min(max(hi, 0), 32)) & ~low_bits((uint32_t)min(max(lo, 0), 32));
+}
+
+// One lane owns one (v row, u block) piece: it walks the block's K/4 16-byte units in the order
+// (lane + p) mod (K/4), so at every step the 32 lanes of a warp hit each 16-byte bank group
+// exactly 32/(K/4) times whatever rows they read.
 template <int NB, int K>
 __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
     using G = Geo<K>;
-    constexpr int WPL = 4;
-    constexpr int LPV = K / WPL;          // lanes per v row
-    constexpr int VPW = 32 / LPV;         // v rows per warp step
+    constexpr int U = G::U;
     extern __shared__ uint4 smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const MatchSmem L(a.total_rows, K, NB, a.stage, a.tmax, a.ng, nwarps);
+    const MatchSmem L(a.total_rows, K, NB, a.tmax, a.ng, nwarps);
     char *base = (char *)smem;
     uint4 *rows = (uint4 *)(base + L.rows);
     uint64_t *us_s = (uint64_t *)(base + L.us);
-    VRec *recs = (VRec *)(base + L.recs);
-    uint64_t *queue = (uint64_t *)(base + L.queue) + warp * QCAP;
+    QEntry *queue = (QEntry *)(base + L.queue) + warp * QCAP;
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
     uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ng+2): groups 1..ng, outputs
     const uint32_t stride = a.ng + 2;
-    const uint32_t gsel = lane / LPV, sub = lane % LPV;
-    const uint32_t stage = a.stage;
     const uint32_t lanes_below = (1u << lane) - 1u;
 
     for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = a.pat[i];
@@ -369,23 +376,15 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
     }
     const bool c2_live = NB == 8 || (NB > 4 && NB == (int)a.nres);
 
-    auto issue = [&](uint64_t from, uint64_t count, uint32_t buf) {
-        const char *src = (const char *)(a.rec + from);
-        char *dst = (char *)(recs + (size_t)buf * stage);
-        for (uint32_t k = threadIdx.x; k < count * 2; k += blockDim.x) cp_async16(dst + 16 * k, src + 16 * k);
-        cp_async_commit();
-    };
-
     for (uint64_t it = i0; it < i1; ++it) {
         while (a.item_prefix[bsearch + 1] <= it) ++bsearch;  // items are visited in order
         const uint64_t b = bsearch;
-        const uint2 range = a.bv[b];
+        const uint4 range = a.bv[b];
         const uint64_t va = range.x + (it - a.item_prefix[b]) * vch;
         const uint64_t vb = umin64(range.y, va + vch);
+        const uint64_t f0 = range.z, f1 = range.w;        // rows covering the whole block
         const uint32_t block_u0 = (uint32_t)(b * G::UB);
         __syncthreads();                                  // previous item finished with shared memory
-        const uint64_t nch = (vb - va + stage - 1) / stage;
-        issue(va, umin64(stage, vb - va), 0);             // first chunk of records overlaps the row build
         if (b != cur) {
             for (uint32_t k = threadIdx.x; k < G::UB; k += blockDim.x)
                 us_s[k] = block_u0 + k < a.nu ? a.us[block_u0 + k] : 0;
@@ -394,14 +393,14 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
             cur = b;
         }
         for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) cnt_s[k] = 0;
+        __syncthreads();
         const uint64_t tile_base = tile_of(a.rec[va].v, a.v_first, a.width);
 
         uint32_t c1 = 0, c2 = 0;
         uint64_t ctile = UINT64_MAX, t_lo = 1, t_hi = 0;  // this lane's subtile and its v range
         uint32_t qhead = 0, qtail = 0;                    // warp-uniform ring positions
 
-        // group-1/2 populations of every lane, reduced over lanes of the same subtile
-        auto flush = [&]() {
+        auto flush = [&]() {                              // populations reduced over lanes of a subtile
             const uint64_t key = (c1 | c2) ? ctile : UINT64_MAX - 1 - lane;
             const uint32_t same = __match_any_sync(0xffffffffu, key);
             const uint32_t s1 = __reduce_add_sync(same, c1), s2 = __reduce_add_sync(same, c2);
@@ -418,29 +417,26 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
             c1 = c2 = 0;
         };
 
-        // Exact later filters on up to 32 queued survivors, one per lane.
-        auto drain = [&](uint32_t n, const VRec *cb) {
+        auto drain = [&](uint32_t n) {                    // exact later filters, one queued survivor per lane
             __syncwarp();
             const bool mine = lane < n;
-            const uint64_t e = mine ? queue[(qhead + lane) & (QCAP - 1)] : 0;
+            QEntry e{0, 0, 0};
+            if (mine) e = queue[(qhead + lane) & (QCAP - 1)];
             __syncwarp();
             qhead += n;
             bool pass = false;
             u128 x{0, 0};
-            uint64_t tile = 0;
+            const uint64_t tile = tile_base + e.slot;
             if (mine) {
-                const uint32_t uidx = (uint32_t)(e & 0xffff), vloc = (uint32_t)((e >> 16) & 0xffff);
-                const uint64_t slot = e >> 32;
-                tile = tile_base + slot;
-                const u128 pos = mul_wide(us_s[uidx], a.B), shift = mul_wide(cb[vloc].v, a.A);
-                uint32_t *cs = slot < a.tmax ? cnt_s + slot * stride : nullptr;
+                uint32_t *cs = e.slot < a.tmax ? cnt_s + e.slot * stride : nullptr;
+                const u128 pos = mul_wide(us_s[e.uidx], a.B), shift = mul_wide(e.v, a.A);
                 if (less128(pos, shift)) {
                     atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 2], 1ull);
                 } else {
                     x = sub128(pos, shift);
-                    uint32_t h[6] = {(uint32_t)x.lo & 0xffffu, (uint32_t)(x.lo >> 16) & 0xffffu,
-                                     (uint32_t)(x.lo >> 32) & 0xffffu, (uint32_t)(x.lo >> 48),
-                                     (uint32_t)x.hi & 0xffffu, (uint32_t)(x.hi >> 16) & 0xffffu};
+                    const uint32_t h[6] = {(uint32_t)x.lo & 0xffffu, (uint32_t)(x.lo >> 16) & 0xffffu,
+                                           (uint32_t)(x.lo >> 32) & 0xffffu, (uint32_t)(x.lo >> 48),
+                                           (uint32_t)x.hi & 0xffffu, (uint32_t)(x.hi >> 16) & 0xffffu};
                     pass = true;
                     for (uint32_t idx = NB; idx < a.nres; ++idx) {
                         const FiltC f = a.fcs[idx];
@@ -463,11 +459,12 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
             }
             const uint32_t won = __ballot_sync(0xffffffffu, pass);
             if (won) {
-                unsigned long long base_slot = 0;
-                if (lane == (uint32_t)(__ffs(won) - 1)) base_slot = atomicAdd(a.n_out, (unsigned long long)__popc(won));
-                base_slot = __shfl_sync(0xffffffffu, base_slot, __ffs(won) - 1);
+                const uint32_t leader = __ffs(won) - 1;
+                unsigned long long first = 0;
+                if (lane == leader) first = atomicAdd(a.n_out, (unsigned long long)__popc(won));
+                first = __shfl_sync(0xffffffffu, first, leader);
                 if (pass) {
-                    const unsigned long long o = base_slot + __popc(won & lanes_below);
+                    const unsigned long long o = first + __popc(won & lanes_below);
                     if (o < a.out_cap) {
                         a.out[2 * o] = x.lo;
                         a.out[2 * o + 1] = x.hi | (tile << 32);
@@ -476,62 +473,67 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
             }
         };
 
-        for (uint64_t ch = 0; ch < nch; ++ch) {
-            const uint64_t cstart = va + ch * stage;
-            const uint32_t cn = (uint32_t)umin64(stage, vb - cstart);
-            if (ch + 1 < nch) issue(cstart + stage, umin64(stage, vb - cstart - stage), (uint32_t)((ch + 1) & 1));
-            else cp_async_commit();
-            cp_async_wait1();
-            __syncthreads();
-            const VRec *cb = recs + (size_t)(ch & 1) * stage;
-
-            for (uint32_t v0 = warp * VPW; v0 < cn; v0 += nwarps * VPW) {
-                const uint32_t vloc = v0 + gsel;
-                const bool active = vloc < cn;
-                const VRec r = cb[active ? vloc : 0];
-                const int32_t lb = sub * WPL * 32;
-                int32_t ls = 0, le = 0;
-                if (active) {
-                    const int32_t s = max((int32_t)(r.left - block_u0), 0);   // indices < 2^31
-                    const int32_t e = min((int32_t)(r.right - block_u0), (int32_t)G::UB);
-                    ls = min(max(s - lb, 0), WPL * 32);
-                    le = min(max(e - lb, 0), WPL * 32);
-                    le = max(le, ls);
+        const uint64_t nrounds = (vb - va + 31) / 32;
+        VRec next;
+        {
+            const uint64_t vi = va + (uint64_t)warp * 32 + lane;
+            if (warp < nrounds && vi < vb) next = a.rec[vi];
+        }
+        for (uint64_t r = warp; r < nrounds; r += nwarps) {
+            const uint64_t v_round = va + r * 32;
+            const uint64_t vi = v_round + lane;
+            const bool active = vi < vb;
+            const VRec rec = next;
+            {
+                const uint64_t vn = vi + (uint64_t)nwarps * 32;
+                if (r + nwarps < nrounds && vn < vb) next = a.rec[vn];   // prefetch one round ahead
+            }
+            const bool full = v_round >= f0 && v_round + 32 <= f1;       // warp-uniform
+            int32_t s = 0, e = 0;                                         // piece as bits of the block
+            if (active) {
+                s = max((int32_t)(rec.left - block_u0), 0);
+                e = min((int32_t)(rec.right - block_u0), (int32_t)G::UB);
+                e = max(e, s);
+            }
+            const bool moved = active && (rec.v < t_lo || rec.v >= t_hi);
+            if (__any_sync(0xffffffffu, moved)) {
+                flush();
+                if (moved) {
+                    ctile = tile_of(rec.v, a.v_first, a.width);
+                    t_lo = a.v_first + ctile * a.width;
+                    t_hi = t_lo + a.width;
                 }
-                uint4 acc = rows[G::unit(r.row[0], sub)];
+            }
+            const uint4 *rb[NB];
+#pragma unroll
+            for (int f = 0; f < NB; ++f) rb[f] = rows + (uint32_t)(active ? rec.row[f] : a.row0[f]) * U;
+            const uint32_t slot = (uint32_t)(ctile - tile_base);
+
+#pragma unroll
+            for (int p = 0; p < U; ++p) {
+                const uint32_t u = (lane + p) & (U - 1);
+                uint4 acc = rb[0][u];
                 uint4 acc4;
 #pragma unroll
                 for (int f = 1; f < NB; ++f) {
                     if (f == 4) acc4 = acc;
-                    const uint4 w = rows[G::unit(r.row[f], sub)];
+                    const uint4 w = rb[f][u];
                     acc.x &= w.x;
                     acc.y &= w.y;
                     acc.z &= w.z;
                     acc.w &= w.w;
                 }
                 if (NB <= 4) acc4 = acc;
-                if (ls > 0 || le < WPL * 32) {
-                    const uint32_t m0 = low_bits((uint32_t)min(max(le, 0), 32)) & ~low_bits((uint32_t)min(max(ls, 0), 32));
-                    const uint32_t m1 = low_bits((uint32_t)min(max(le - 32, 0), 32)) & ~low_bits((uint32_t)min(max(ls - 32, 0), 32));
-                    const uint32_t m2 = low_bits((uint32_t)min(max(le - 64, 0), 32)) & ~low_bits((uint32_t)min(max(ls - 64, 0), 32));
-                    const uint32_t m3 = low_bits((uint32_t)min(max(le - 96, 0), 32)) & ~low_bits((uint32_t)min(max(ls - 96, 0), 32));
+                if (!full) {
+                    const int32_t lo = s - (int32_t)u * 128, hi = e - (int32_t)u * 128;
+                    const uint32_t m0 = unit_mask(lo, hi), m1 = unit_mask(lo - 32, hi - 32);
+                    const uint32_t m2 = unit_mask(lo - 64, hi - 64), m3 = unit_mask(lo - 96, hi - 96);
                     acc.x &= m0, acc.y &= m1, acc.z &= m2, acc.w &= m3;
                     acc4.x &= m0, acc4.y &= m1, acc4.z &= m2, acc4.w &= m3;
                 }
-                const bool moved = active && (r.v < t_lo || r.v >= t_hi);
-                if (__any_sync(0xffffffffu, moved)) {
-                    flush();
-                    if (moved) {
-                        ctile = tile_of(r.v, a.v_first, a.width);
-                        t_lo = a.v_first + ctile * a.width;
-                        t_hi = t_lo + a.width;
-                    }
-                }
                 c1 += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
                 if (c2_live) c2 += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
-
                 uint64_t sl = (uint64_t)acc.y << 32 | acc.x, sh = (uint64_t)acc.w << 32 | acc.z;
-                const uint32_t slot = (uint32_t)(ctile - tile_base);
                 while (__any_sync(0xffffffffu, (sl | sh) != 0)) {
                     const bool has = (sl | sh) != 0;
                     const uint32_t bal = __ballot_sync(0xffffffffu, has);
@@ -544,16 +546,18 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
                             bit = 64 + __ffsll(sh) - 1;
                             sh &= sh - 1;
                         }
-                        const uint32_t pos = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
-                        queue[pos] = (uint64_t)(lb + bit) | ((uint64_t)vloc << 16) | ((uint64_t)slot << 32);
+                        QEntry q;
+                        q.v = rec.v;
+                        q.uidx = u * 128 + bit;
+                        q.slot = slot;
+                        queue[(qtail + __popc(bal & lanes_below)) & (QCAP - 1)] = q;
                     }
                     qtail += __popc(bal);
-                    if (qtail - qhead >= 32) drain(32, cb);
+                    if (qtail - qhead >= 32) drain(32);
                 }
             }
-            if (qtail != qhead) drain(qtail - qhead, cb);  // records of this chunk are about to be replaced
-            __syncthreads();                              // buffer (ch & 1) is refilled at chunk ch + 2
         }
+        if (qtail != qhead) drain(qtail - qhead);
         flush();
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) {
@@ -763,7 +767,7 @@ extern "C" int pc_filters_free(pc_ctx *ctx, pc_filters *f) {
 namespace {
 
 struct Tuned {
-    uint32_t nb, K, threads, stage;
+    uint32_t nb, K, threads;
     uint64_t v_chunk;
 };
 
@@ -781,15 +785,12 @@ Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
     if (optin <= 0) optin = 227 * 1024;
     for (;;) {
-        for (uint32_t stage = 512; stage >= 64; stage /= 2) {
-            for (uint32_t tmax = TMAX_DEFAULT; tmax >= 4; tmax /= 2) {
-                MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, stage, tmax, f->ng, r.threads / 32);
-                if (L.total <= (uint32_t)optin) {
-                    r.stage = stage;
-                    *tmax_out = tmax;
-                    *smem_out = L.total;
-                    return r;
-                }
+        for (uint32_t tmax = TMAX_DEFAULT; tmax >= 4; tmax /= 2) {
+            MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, tmax, f->ng, r.threads / 32);
+            if (L.total <= (uint32_t)optin) {
+                *tmax_out = tmax;
+                *smem_out = L.total;
+                return r;
             }
         }
         if (r.K > 16) r.K /= 2;
@@ -823,7 +824,7 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
     uint64_t *d_counts, *d_geo, *d_out, *d_prefix, *d_vchunk, *d_pieces;
     unsigned long long *d_nout, *d_bad;
     VRec *d_rec;
-    uint2 *d_bv;
+    uint4 *d_bv;
     const uint32_t UB = tn.K * 32;
     const uint64_t nblocks = (nu + UB - 1) / UB;
     int rc = s.get(&d_counts, (uint64_t)ntiles * stride);
@@ -928,7 +929,6 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
         ma.vchunk = d_vchunk;
         ma.v_first = v_first;
         ma.width = width;
-        ma.stage = tn.stage;
         for (uint32_t i = 0; i < f->nres && i < (uint32_t)FC_INLINE; ++i) ma.fcs[i] = f->fcs[i];
         PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
         if (tn.K == 16) rc = launch_match_k<16>(ctx, ma, smem, tn.threads, grid);
