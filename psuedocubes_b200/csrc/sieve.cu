@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
                 if (slot < a.tmax) {
                     if (s1) atomicAdd(cnt_s + slot * stride + 1, s1);
                     if (s2) atomicAdd(cnt_s + slot * stride + 2, s2);
-                } else {
+                } else if (ctile < a.ntiles) {
                     if (s1) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 1], (unsigned long long)s1);
                     if (s2) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 2], (unsigned long long)s2);
                 }
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
             bool pass = false;
             u128 x{0, 0};
             const uint64_t tile = tile_base + e.slot;
-            if (mine) {
+            if (mine && tile < a.ntiles) {
                 uint32_t *cs = e.slot < a.tmax ? cnt_s + e.slot * stride : nullptr;
                 const u128 pos = mul_wide(us_s[e.uidx], a.B), shift = mul_wide(e.v, a.A);
                 if (less128(pos, shift)) {
@@ -488,7 +488,8 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
                 const uint64_t vn = vi + (uint64_t)nwarps * 32;
                 if (r + nwarps < nrounds && vn < vb) next = a.rec[vn];   // prefetch one round ahead
             }
-            const bool full = v_round >= f0 && v_round + 32 <= f1;       // warp-uniform
+            // warp-uniform: all 32 rows exist in this item and cover the whole block
+            const bool full = v_round >= f0 && v_round + 32 <= umin64(f1, vb);
             int32_t s = 0, e = 0;                                         // piece as bits of the block
             if (active) {
                 s = max((int32_t)(rec.left - block_u0), 0);
