@@ -307,23 +307,20 @@ __device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, const u
     }
 }
 
-constexpr int QCAP = 64;   // survivor ring per warp (pending < 64 by construction)
+constexpr int QCAP = 64;              // survivor ring per warp (pending < 64 by construction)
+constexpr uint32_t SLOT_FAR = 0xFFFFF;  // queued slot too large to encode: the drain recomputes it
 
-struct QEntry {
-    uint64_t v;
-    uint32_t uidx;             // u index within the block
-    uint32_t slot;             // subtile - first subtile of the item
-};
-
-// Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.
+// Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.  The
+// survivor ring is stored as arrays: v (8 bytes) and (u index | slot << 12) (4 bytes).
 struct MatchSmem {
-    uint32_t rows, us, queue, pat, cnt, total;
+    uint32_t rows, us, qv, qm, pat, cnt, total;
     __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t tmax, uint32_t ng,
                                   uint32_t warps) {
         rows = 0;
         us = rows + total_rows * (K / 4) * 16;
-        queue = us + K * 32 * 8;
-        pat = queue + warps * QCAP * (uint32_t)sizeof(QEntry);
+        qv = us + K * 32 * 8;
+        qm = qv + warps * QCAP * 8;
+        pat = qm + warps * QCAP * 4;
         cnt = pat + nb * PATW * 4;
         total = cnt + tmax * (ng + 2) * 4;
     }
@@ -346,14 +343,15 @@ __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bit
 template <int NB, int K>
 __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
     using G = Geo<K>;
-    constexpr int U = G::U;
+    constexpr uint32_t U = G::U;
     extern __shared__ uint4 smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const MatchSmem L(a.total_rows, K, NB, a.tmax, a.ng, nwarps);
     char *base = (char *)smem;
-    uint4 *rows = (uint4 *)(base + L.rows);
+    const uint4 *rows = (const uint4 *)(base + L.rows);
     uint64_t *us_s = (uint64_t *)(base + L.us);
-    QEntry *queue = (QEntry *)(base + L.queue) + warp * QCAP;
+    uint64_t *qv = (uint64_t *)(base + L.qv) + warp * QCAP;
+    uint32_t *qm = (uint32_t *)(base + L.qm) + warp * QCAP;
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
     uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ng+2): groups 1..ng, outputs
     const uint32_t stride = a.ng + 2;
@@ -381,15 +379,17 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
         const uint64_t b = bsearch;
         const uint4 range = a.bv[b];
         const uint64_t va = range.x + (it - a.item_prefix[b]) * vch;
-        const uint64_t vb = umin64(range.y, va + vch);
-        const uint64_t f0 = range.z, f1 = range.w;        // rows covering the whole block
+        const uint32_t nv_item = (uint32_t)(umin64(range.y, va + vch) - va);   // <= 2^20
+        // rows of this item covering the whole block, relative to va
+        const uint32_t full_lo = (uint32_t)(range.z > va ? umin64(range.z - va, nv_item) : 0);
+        const uint32_t full_hi = (uint32_t)(range.w > va ? umin64(range.w - va, nv_item) : 0);
         const uint32_t block_u0 = (uint32_t)(b * G::UB);
         __syncthreads();                                  // previous item finished with shared memory
         if (b != cur) {
             for (uint32_t k = threadIdx.x; k < G::UB; k += blockDim.x)
                 us_s[k] = block_u0 + k < a.nu ? a.us[block_u0 + k] : 0;
             __syncthreads();
-            build_rows<NB, K>(a, rows, us_s, pat_s, block_u0, lane, warp, nwarps);
+            build_rows<NB, K>(a, (uint4 *)rows, us_s, pat_s, block_u0, lane, warp, nwarps);
             cur = b;
         }
         for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) cnt_s[k] = 0;
@@ -420,16 +420,21 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
         auto drain = [&](uint32_t n) {                    // exact later filters, one queued survivor per lane
             __syncwarp();
             const bool mine = lane < n;
-            QEntry e{0, 0, 0};
-            if (mine) e = queue[(qhead + lane) & (QCAP - 1)];
+            uint64_t v = 0;
+            uint32_t meta = 0;
+            if (mine) {
+                v = qv[(qhead + lane) & (QCAP - 1)];
+                meta = qm[(qhead + lane) & (QCAP - 1)];
+            }
             __syncwarp();
             qhead += n;
             bool pass = false;
             u128 x{0, 0};
-            const uint64_t tile = tile_base + e.slot;
+            const uint32_t slot = meta >> 12;
+            const uint64_t tile = slot == SLOT_FAR ? tile_of(v, a.v_first, a.width) : tile_base + slot;
             if (mine && tile < a.ntiles) {
-                uint32_t *cs = e.slot < a.tmax ? cnt_s + e.slot * stride : nullptr;
-                const u128 pos = mul_wide(us_s[e.uidx], a.B), shift = mul_wide(e.v, a.A);
+                uint32_t *cs = slot < a.tmax ? cnt_s + slot * stride : nullptr;
+                const u128 pos = mul_wide(us_s[meta & 0xfff], a.B), shift = mul_wide(v, a.A);
                 if (less128(pos, shift)) {
                     atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 2], 1ull);
                 } else {
@@ -473,24 +478,18 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
             }
         };
 
-        const uint64_t nrounds = (vb - va + 31) / 32;
+        const uint32_t nrounds = (nv_item + 31) / 32;
         VRec next;
-        {
-            const uint64_t vi = va + (uint64_t)warp * 32 + lane;
-            if (warp < nrounds && vi < vb) next = a.rec[vi];
-        }
-        for (uint64_t r = warp; r < nrounds; r += nwarps) {
-            const uint64_t v_round = va + r * 32;
-            const uint64_t vi = v_round + lane;
-            const bool active = vi < vb;
+        if (warp < nrounds && warp * 32 + lane < nv_item) next = a.rec[va + warp * 32 + lane];
+        for (uint32_t r = warp; r < nrounds; r += nwarps) {
+            const uint32_t rel = r * 32 + lane;
+            const bool active = rel < nv_item;
             const VRec rec = next;
-            {
-                const uint64_t vn = vi + (uint64_t)nwarps * 32;
-                if (r + nwarps < nrounds && vn < vb) next = a.rec[vn];   // prefetch one round ahead
-            }
-            // warp-uniform: all 32 rows exist in this item and cover the whole block
-            const bool full = v_round >= f0 && v_round + 32 <= umin64(f1, vb);
-            int32_t s = 0, e = 0;                                         // piece as bits of the block
+            if (r + nwarps < nrounds && rel + nwarps * 32 < nv_item)
+                next = a.rec[va + rel + nwarps * 32];     // prefetch one round ahead
+            // warp-uniform: all 32 rows exist and cover the whole block
+            const bool full = r * 32 >= full_lo && r * 32 + 32 <= full_hi;
+            int32_t s = 0, e = 0;                         // piece as bits of the block
             if (active) {
                 s = max((int32_t)(rec.left - block_u0), 0);
                 e = min((int32_t)(rec.right - block_u0), (int32_t)G::UB);
@@ -505,20 +504,21 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
                     t_hi = t_lo + a.width;
                 }
             }
-            const uint4 *rb[NB];
+            uint32_t ro[NB];                              // unit offset of each filter's row
 #pragma unroll
-            for (int f = 0; f < NB; ++f) rb[f] = rows + (uint32_t)(active ? rec.row[f] : a.row0[f]) * U;
-            const uint32_t slot = (uint32_t)(ctile - tile_base);
+            for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)(active ? rec.row[f] : a.row0[f]) * U;
+            const uint64_t slot64 = ctile - tile_base;
+            const uint32_t meta_hi = (slot64 < SLOT_FAR ? (uint32_t)slot64 : SLOT_FAR) << 12;
 
-#pragma unroll
-            for (int p = 0; p < U; ++p) {
+#pragma unroll 1
+            for (uint32_t p = 0; p < U; ++p) {
                 const uint32_t u = (lane + p) & (U - 1);
-                uint4 acc = rb[0][u];
+                uint4 acc = rows[ro[0] + u];
                 uint4 acc4;
 #pragma unroll
                 for (int f = 1; f < NB; ++f) {
                     if (f == 4) acc4 = acc;
-                    const uint4 w = rb[f][u];
+                    const uint4 w = rows[ro[f] + u];
                     acc.x &= w.x;
                     acc.y &= w.y;
                     acc.z &= w.z;
@@ -534,24 +534,27 @@ __global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
                 }
                 c1 += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
                 if (c2_live) c2 += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
-                uint64_t sl = (uint64_t)acc.y << 32 | acc.x, sh = (uint64_t)acc.w << 32 | acc.z;
-                while (__any_sync(0xffffffffu, (sl | sh) != 0)) {
-                    const bool has = (sl | sh) != 0;
+                while (__any_sync(0xffffffffu, (acc.x | acc.y | acc.z | acc.w) != 0)) {
+                    const bool has = (acc.x | acc.y | acc.z | acc.w) != 0;
                     const uint32_t bal = __ballot_sync(0xffffffffu, has);
                     if (has) {
                         uint32_t bit;
-                        if (sl) {
-                            bit = __ffsll(sl) - 1;
-                            sl &= sl - 1;
+                        if (acc.x) {
+                            bit = __ffs(acc.x) - 1;
+                            acc.x &= acc.x - 1;
+                        } else if (acc.y) {
+                            bit = 32 + __ffs(acc.y) - 1;
+                            acc.y &= acc.y - 1;
+                        } else if (acc.z) {
+                            bit = 64 + __ffs(acc.z) - 1;
+                            acc.z &= acc.z - 1;
                         } else {
-                            bit = 64 + __ffsll(sh) - 1;
-                            sh &= sh - 1;
+                            bit = 96 + __ffs(acc.w) - 1;
+                            acc.w &= acc.w - 1;
                         }
-                        QEntry q;
-                        q.v = rec.v;
-                        q.uidx = u * 128 + bit;
-                        q.slot = slot;
-                        queue[(qtail + __popc(bal & lanes_below)) & (QCAP - 1)] = q;
+                        const uint32_t at = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
+                        qv[at] = rec.v;
+                        qm[at] = (u * 128 + bit) | meta_hi;
                     }
                     qtail += __popc(bal);
                     if (qtail - qhead >= 32) drain(32);
