@@ -210,7 +210,7 @@ class FusedMatcher:
 class MaskedMatcher(FusedMatcher):
     """Residue bitsets of the first residual filters intersected before any wide construction
     (pseudocube/batch_experiment.py:170-254); the production engine."""
-    bitset_filters = 6
+    bitset_filters = 7
     lease_output_records = 1 << 20
 
     def __init__(self, runtime: Runtime, config: Config, tuning: dict[str, int] | None = None) -> None:

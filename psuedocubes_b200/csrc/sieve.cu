@@ -778,7 +778,7 @@ struct Tuned {
 Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_t *smem_out, uint32_t *tmax_out) {
     Tuned r{};
     uint32_t nb_min = std::min<uint32_t>(f->nres, 4);
-    r.nb = t && t->bitset_filters ? t->bitset_filters : std::min<uint32_t>(f->nbmax, 6);
+    r.nb = t && t->bitset_filters ? t->bitset_filters : std::min<uint32_t>(f->nbmax, 7);
     r.nb = std::max(nb_min, std::min(r.nb, f->nbmax));
     r.K = t && t->block_words ? t->block_words : 32;
     if (r.K != 16 && r.K != 32 && r.K != 64) r.K = 32;
