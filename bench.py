@@ -169,7 +169,8 @@ def run_ours(args) -> None:
     runtime = Runtime(time.monotonic() + 7200, 16 * 1024**3, 0.5, device=local)
     config = Config(619, 10**27, 3 * 10**27, A619, B619)
     af, bf = (GPUFocus(runtime, f) for f in config.focuses())
-    tuning = {k: v for k, v in (('bitset_filters', args.bitset_filters), ('block_words', args.block_words)) if v}
+    tuning = {k: v for k, v in (('bitset_filters', args.bitset_filters), ('block_words', args.block_words),
+                                ('threads', args.threads)) if v}
     matcher = MaskedMatcher(runtime, config, tuning)
     width = PROFILE['tile_width']
     nt = args.lease_batches * 64
@@ -183,12 +184,16 @@ def run_ours(args) -> None:
     lib, ctx = runtime.lib, runtime.ctx
     c = config
 
+    effective: dict = {}
+
     def step(index: int) -> tuple[int, dict]:
         first, end = lease_bounds(index * world + rank, args.lease_batches)
         runtime.call(lib.pc_run_lease(ctx, af.handle, bf.handle, matcher.filters.handle, ctypes.byref(matcher.tuning),
                                       first, end, width, c.lo & MASK, c.lo >> 64, c.hi & MASK, c.hi >> 64, counts,
                                       geometry, records, cap, ctypes.byref(n_out), ctypes.byref(stats)))
-        return int(counts.reshape(nt, ng + 3)[:, 0].sum()), stats.as_dict()
+        info = stats.as_dict()
+        effective.update({k: info[k] for k in ('bitset_filters', 'block_words', 'threads')})
+        return int(counts.reshape(nt, ng + 3)[:, 0].sum()), info
 
     for k in range(args.warmup):
         step(k)
@@ -238,7 +243,7 @@ def run_ours(args) -> None:
                                   peak_basis=f'{runtime.sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz'),
                     e2e=dict(value=e2e_positions * world / e2e_seconds if e2e_seconds else None, unit=UNIT, h2d_bytes_per_step=0,
                              d2h_bytes_per_step=int(d2h), api='psuedocubes_b200.optimized.compute_lease'),
-                    gpu_launches=launches, clocks=clock, tuning=tuning or 'default',
+                    gpu_launches=launches, clocks=clock, tuning=effective,
                     kernel_ms_per_step=kernel_ms / args.steps)
         if world == 1 and not args.no_cpu:
             line['cpu_baseline'] = {k: v for k, v in cpu_sample(1, args.warmup, batches=8).items()
@@ -262,6 +267,7 @@ def main() -> None:
     parser.add_argument('--e2e-steps', type=int, default=2)
     parser.add_argument('--bitset-filters', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--block-words', type=int, default=0, help='tuning override (0 = library default)')
+    parser.add_argument('--threads', type=int, default=0, help='tuning override (0 = library default)')
     args = parser.parse_args()
     if args.impl == 'reference':
         run_reference(args)

@@ -100,7 +100,7 @@ typedef struct pc_stats {
     uint64_t work_items;
     uint64_t outputs;
     uint64_t launches;         /* kernels launched by the call */
-    uint64_t reserved[5];
+    uint64_t reserved[5];      /* [0..2]: bitset filters, block words and threads the call used */
 } pc_stats;
 
 /*

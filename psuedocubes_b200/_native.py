@@ -41,7 +41,9 @@ class Stats(ctypes.Structure):
 
     def as_dict(self) -> dict[str, Any]:
         return dict(kernel_ms=self.kernel_ms, bounds_ms=self.bounds_ms, window_ms=self.window_ms,
-                    total_ms=self.total_ms, outputs=int(self.outputs), launches=int(self.launches))
+                    total_ms=self.total_ms, outputs=int(self.outputs), launches=int(self.launches),
+                    bitset_filters=int(self.reserved[0]), block_words=int(self.reserved[1]),
+                    threads=int(self.reserved[2]))
 
 
 _P = ctypes.c_void_p

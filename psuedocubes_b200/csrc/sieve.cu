@@ -340,8 +340,8 @@ __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bit
 // One lane owns one (v row, u block) piece: it walks the block's K/4 16-byte units in the order
 // (lane + p) mod (K/4), so at every step the 32 lanes of a warp hit each 16-byte bank group
 // exactly 32/(K/4) times whatever rows they read.
-template <int NB, int K>
-__global__ void __launch_bounds__(512, 1) k_match(const MatchArgs a) {
+template <int NB, int K, int NT>
+__global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     using G = Geo<K>;
     constexpr uint32_t U = G::U;
     extern __shared__ uint4 smem[];
@@ -635,29 +635,36 @@ __global__ void __launch_bounds__(256) k_plain(const PlainArgs a) {
         if (k != a.ng + 1 && cnt[k]) atomicAdd((unsigned long long *)&a.counts[k], cnt[k]);
 }
 
-template <int NB, int K>
-int launch_match_t(pc_ctx *ctx, const MatchArgs &a, size_t smem, int threads, int grid) {
-    auto kern = k_match<NB, K>;
+template <int NB, int K, int NT>
+int launch_match_t(pc_ctx *ctx, const MatchArgs &a, size_t smem, int grid) {
+    auto kern = k_match<NB, K, NT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return pc_cuda_fail(ctx, e, "match smem attribute");
-    kern<<<grid, threads, smem, ctx->stream>>>(a);
+    kern<<<grid, NT, smem, ctx->stream>>>(a);
     PC_LAUNCHED(ctx, "match");
     return PC_OK;
 }
 
-template <int K>
-int launch_match_k(pc_ctx *ctx, const MatchArgs &a, size_t smem, int threads, int grid) {
+template <int K, int NT>
+int launch_match_k(pc_ctx *ctx, const MatchArgs &a, size_t smem, int grid) {
     switch (a.nb) {
-        case 1: return launch_match_t<1, K>(ctx, a, smem, threads, grid);
-        case 2: return launch_match_t<2, K>(ctx, a, smem, threads, grid);
-        case 3: return launch_match_t<3, K>(ctx, a, smem, threads, grid);
-        case 4: return launch_match_t<4, K>(ctx, a, smem, threads, grid);
-        case 5: return launch_match_t<5, K>(ctx, a, smem, threads, grid);
-        case 6: return launch_match_t<6, K>(ctx, a, smem, threads, grid);
-        case 7: return launch_match_t<7, K>(ctx, a, smem, threads, grid);
-        case 8: return launch_match_t<8, K>(ctx, a, smem, threads, grid);
+        case 1: return launch_match_t<1, K, NT>(ctx, a, smem, grid);
+        case 2: return launch_match_t<2, K, NT>(ctx, a, smem, grid);
+        case 3: return launch_match_t<3, K, NT>(ctx, a, smem, grid);
+        case 4: return launch_match_t<4, K, NT>(ctx, a, smem, grid);
+        case 5: return launch_match_t<5, K, NT>(ctx, a, smem, grid);
+        case 6: return launch_match_t<6, K, NT>(ctx, a, smem, grid);
+        case 7: return launch_match_t<7, K, NT>(ctx, a, smem, grid);
+        case 8: return launch_match_t<8, K, NT>(ctx, a, smem, grid);
     }
     return pc_fail(ctx, PC_INVALID, "unsupported bitset filter count");
+}
+
+template <int NT>
+int launch_match_n(pc_ctx *ctx, const MatchArgs &a, uint32_t K, size_t smem, int grid) {
+    if (K == 16) return launch_match_k<16, NT>(ctx, a, smem, grid);
+    if (K == 32) return launch_match_k<32, NT>(ctx, a, smem, grid);
+    return launch_match_k<64, NT>(ctx, a, smem, grid);
 }
 
 uint32_t inv_mod(uint32_t a, uint32_t q) {
@@ -782,8 +789,9 @@ Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_
     r.nb = std::max(nb_min, std::min(r.nb, f->nbmax));
     r.K = t && t->block_words ? t->block_words : 32;
     if (r.K != 16 && r.K != 32 && r.K != 64) r.K = 32;
-    r.threads = t && t->threads ? t->threads : 512;
-    if (r.threads != 256 && r.threads != 512) r.threads = 512;
+    const bool fixed_threads = t && t->threads;
+    r.threads = fixed_threads ? t->threads : 1024;
+    if (r.threads != 512 && r.threads != 768 && r.threads != 1024) r.threads = 512;
     r.v_chunk = t ? t->v_chunk : 0;
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
@@ -797,7 +805,8 @@ Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_
                 return r;
             }
         }
-        if (r.K > 16) r.K /= 2;
+        if (!fixed_threads && r.threads > 512) r.threads = r.threads == 1024 ? 768 : 512;
+        else if (r.K > 16) r.K /= 2;
         else if (r.nb > nb_min) r.nb--;
         else {
             *smem_out = 0;
@@ -935,9 +944,9 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
         ma.width = width;
         for (uint32_t i = 0; i < f->nres && i < (uint32_t)FC_INLINE; ++i) ma.fcs[i] = f->fcs[i];
         PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
-        if (tn.K == 16) rc = launch_match_k<16>(ctx, ma, smem, tn.threads, grid);
-        else if (tn.K == 32) rc = launch_match_k<32>(ctx, ma, smem, tn.threads, grid);
-        else rc = launch_match_k<64>(ctx, ma, smem, tn.threads, grid);
+        if (tn.threads == 1024) rc = launch_match_n<1024>(ctx, ma, tn.K, smem, grid);
+        else if (tn.threads == 768) rc = launch_match_n<768>(ctx, ma, tn.K, smem, grid);
+        else rc = launch_match_n<512>(ctx, ma, tn.K, smem, grid);
         if (rc) return rc;
         ++launches;
         PC_CHECK(ctx, cudaEventRecord(ctx->ev[3], st));
@@ -954,6 +963,9 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
         io.stats->kernel_ms = run_match ? elapsed_ms(ctx->ev[2], ctx->ev[3]) : 0.0;
         io.stats->outputs = n;
         io.stats->launches = launches;
+        io.stats->reserved[0] = tn.nb;
+        io.stats->reserved[1] = tn.K;
+        io.stats->reserved[2] = tn.threads;
     }
     if (host_nout[1]) return pc_fail(ctx, PC_INVALID, "v row outside the subtile geometry");
     if (n > io.out_cap) return pc_fail(ctx, PC_OVERFLOW, "output overflow; attempt cannot commit");
