@@ -9,6 +9,7 @@
 #define PC_MAX_BITSET 8        // residual filters intersected as bitsets
 #define PC_MAX_RES 1024        // residual filters per (p, A, B)
 #define PC_MAX_WHEEL_T 6       // focus rings handled as wheel bitset rows
+#define PC_MAX_CHEAP 4         // residual filters tested per survivor from u and v residues
 
 // ------------------------------------------------------------------------------------------
 // context, errors, memory accounting

@@ -85,7 +85,30 @@ struct MatchArgs {
     uint64_t nblocks;
     const uint64_t *vchunk;          // device scalar
     uint64_t v_first, width;         // subtile of v = (v - v_first) / width
-    FiltC fcs[FC_INLINE];            // residual filters in order (the first nres are used)
+    // cheap tier: residual filters nb .. nb+nch-1 tested per survivor from residues of u and v
+    uint32_t nch;
+    uint32_t cq[PC_MAX_CHEAP], caq[PC_MAX_CHEAP], cbq[PC_MAX_CHEAP], cbits_off[PC_MAX_CHEAP];
+    ModQ cmq[PC_MAX_CHEAP];
+    uint8_t bgroup[16];              // group ended by filter idx (0 = none), idx < nb + nch
+    // deep tier: survivors of every cheap filter, appended to this CTA's slice
+    uint4 *deep;                     // (v lo, v hi, u index, subtile) records
+    uint32_t deep_cap;               // records per CTA slice
+    uint32_t *deep_count;            // per CTA (may exceed deep_cap: the caller retries larger)
+};
+
+struct DeepArgs {
+    const uint64_t *us;
+    const uint4 *deep;
+    const uint32_t *deep_count;
+    uint32_t deep_cap, slices;
+    uint64_t A, B;
+    uint32_t first, nres, ng, ntiles;          // filters first .. nres-1 remain
+    const uint32_t *bits;
+    uint64_t *counts;
+    uint64_t *out;
+    uint64_t out_cap;
+    unsigned long long *n_out;
+    FiltC fcs[FC_INLINE];
 };
 
 // first j with us[j] * B > key
@@ -272,10 +295,18 @@ struct Geo {
 };
 
 template <int NB, int K>
-__device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, const uint64_t *__restrict__ us_s,
-                           const uint32_t *__restrict__ pat_s, uint64_t block_u0, uint32_t lane, uint32_t warp,
+__device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, uint16_t *__restrict__ ures,
+                           const uint32_t *__restrict__ pat_s, uint32_t block_u0, uint32_t lane, uint32_t warp,
                            uint32_t nwarps) {
     using G = Geo<K>;
+    const uint64_t *ub = a.us + block_u0;
+    // residues u*B mod q of the cheap-tier filters, one per block entry
+    for (uint32_t k = threadIdx.x; k < G::UB; k += blockDim.x) {
+        const bool valid = block_u0 + k < a.nu;
+        const uint64_t u = valid ? __ldg(ub + k) : 0;
+        for (uint32_t t = 0; t < a.nch; ++t)
+            ures[t * G::UB + k] = (uint16_t)fastmod32(mod64(u, a.cmq[t]) * a.cbq[t], a.cmq[t].c, a.cq[t]);
+    }
     // a warp builds all q rows of one filter for one 16-byte unit (4 words = 128 u)
     for (uint32_t pair = warp; pair < NB * G::U; pair += nwarps) {
         uint32_t f = pair / G::U, c = pair % G::U;
@@ -286,7 +317,7 @@ __device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, const u
         for (int k = 0; k < 4; ++k) {
             uint32_t local = (c * 4 + k) * 32 + lane;
             valid[k] = block_u0 + local < a.nu;
-            uint32_t um = valid[k] ? mod64(us_s[local], a.mq[f]) : 0;
+            uint32_t um = valid[k] ? mod64(__ldg(ub + local), a.mq[f]) : 0;
             t[k] = fastmod32(um * a.ainvb[f], a.mq[f].c, q);
         }
         const uint32_t *p = pat_s + f * PATW;
@@ -307,31 +338,22 @@ __device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, const u
     }
 }
 
-constexpr int QCAP = 64;              // survivor ring per warp (pending < 64 by construction)
-constexpr uint32_t SLOT_FAR = 0xFFFFF;  // queued slot too large to encode: the drain recomputes it
+constexpr int CBW = 64;   // bitmap words per cheap-tier filter (q <= 2047)
 
-// Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.  The
-// survivor ring is stored as arrays: v (8 bytes) and (u index | slot << 12) (4 bytes).
+// Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.
 struct MatchSmem {
-    uint32_t rows, us, qv, qm, pat, cnt, total;
-    __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t tmax, uint32_t ng,
-                                  uint32_t warps) {
+    uint32_t rows, ures, pat, cbits, cnt, misc, total;
+    __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t nch, uint32_t tmax,
+                                  uint32_t ng) {
         rows = 0;
-        us = rows + total_rows * (K / 4) * 16;
-        qv = us + K * 32 * 8;
-        qm = qv + warps * QCAP * 8;
-        pat = qm + warps * QCAP * 4;
-        cnt = pat + nb * PATW * 4;
-        total = cnt + tmax * (ng + 2) * 4;
+        ures = rows + total_rows * (K / 4) * 16;
+        pat = ures + ((nch * K * 32 * 2 + 15) & ~15u);
+        cbits = pat + nb * PATW * 4;
+        cnt = cbits + nch * CBW * 4;
+        misc = cnt + ((tmax * (ng + 2) * 4 + 15) & ~15u);
+        total = misc + 16;
     }
 };
-
-// x mod q for x < 2^96 from its six 16-bit limbs h (h[0] + sum h[k] (2^16k mod q), then one
-// fast remainder; every partial sum stays below 2^32 because q < 2^13).
-__device__ __forceinline__ uint32_t mod_limbs(const uint32_t h[6], const FiltC &f) {
-    uint32_t t = h[0] + h[1] * f.r16[0] + h[2] * f.r16[1] + h[3] * f.r16[2] + h[4] * f.r16[3] + h[5] * f.r16[4];
-    return fastmod32(t, f.c, f.q);
-}
 
 __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bits [lo, hi) of one 32-bit word
     return low_bits((uint32_t)min(max(hi, 0), 32)) & ~low_bits((uint32_t)min(max(lo, 0), 32));
@@ -339,25 +361,31 @@ __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bit
 
 // One lane owns one (v row, u block) piece: it walks the block's K/4 16-byte units in the order
 // (lane + p) mod (K/4), so at every step the 32 lanes of a warp hit each 16-byte bank group
-// exactly 32/(K/4) times whatever rows they read.
+// exactly 32/(K/4) times whatever rows they read.  Group counters of groups 1..3 live in
+// registers (c[0..2]) and are reduced per subtile when a lane's subtile changes.
 template <int NB, int K, int NT>
 __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     using G = Geo<K>;
     constexpr uint32_t U = G::U;
     extern __shared__ uint4 smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const MatchSmem L(a.total_rows, K, NB, a.tmax, a.ng, nwarps);
+    const MatchSmem L(a.total_rows, K, NB, a.nch, a.tmax, a.ng);
     char *base = (char *)smem;
     const uint4 *rows = (const uint4 *)(base + L.rows);
-    uint64_t *us_s = (uint64_t *)(base + L.us);
-    uint64_t *qv = (uint64_t *)(base + L.qv) + warp * QCAP;
-    uint32_t *qm = (uint32_t *)(base + L.qm) + warp * QCAP;
+    uint16_t *ures = (uint16_t *)(base + L.ures);
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
+    uint32_t *cbits = (uint32_t *)(base + L.cbits);
     uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ng+2): groups 1..ng, outputs
+    uint32_t *deep_ctr = (uint32_t *)(base + L.misc);
     const uint32_t stride = a.ng + 2;
-    const uint32_t lanes_below = (1u << lane) - 1u;
 
     for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = a.pat[i];
+    for (uint32_t i = threadIdx.x; i < a.nch * CBW; i += blockDim.x) {
+        const uint32_t t = i / CBW, w = i % CBW;
+        cbits[i] = w * 32 < a.cq[t] ? a.bits[a.cbits_off[t] + w] : 0u;
+    }
+    if (threadIdx.x == 0) *deep_ctr = 0;
+    uint4 *deep_slice = a.deep + (size_t)blockIdx.x * a.deep_cap;
 
     const uint64_t n_items = a.item_prefix[a.nblocks];
     const uint64_t vch = *a.vchunk;
@@ -373,6 +401,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         bsearch = lo;
     }
     const bool c2_live = NB == 8 || (NB > 4 && NB == (int)a.nres);
+    const uint32_t nch = a.nch;
 
     for (uint64_t it = i0; it < i1; ++it) {
         while (a.item_prefix[bsearch + 1] <= it) ++bsearch;  // items are visited in order
@@ -386,95 +415,30 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         const uint32_t block_u0 = (uint32_t)(b * G::UB);
         __syncthreads();                                  // previous item finished with shared memory
         if (b != cur) {
-            for (uint32_t k = threadIdx.x; k < G::UB; k += blockDim.x)
-                us_s[k] = block_u0 + k < a.nu ? a.us[block_u0 + k] : 0;
-            __syncthreads();
-            build_rows<NB, K>(a, (uint4 *)rows, us_s, pat_s, block_u0, lane, warp, nwarps);
+            build_rows<NB, K>(a, (uint4 *)rows, ures, pat_s, block_u0, lane, warp, nwarps);
             cur = b;
         }
         for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) cnt_s[k] = 0;
         __syncthreads();
         const uint64_t tile_base = tile_of(a.rec[va].v, a.v_first, a.width);
 
-        uint32_t c1 = 0, c2 = 0;
+        uint32_t c[3] = {0, 0, 0};
         uint64_t ctile = UINT64_MAX, t_lo = 1, t_hi = 0;  // this lane's subtile and its v range
-        uint32_t qhead = 0, qtail = 0;                    // warp-uniform ring positions
 
         auto flush = [&]() {                              // populations reduced over lanes of a subtile
-            const uint64_t key = (c1 | c2) ? ctile : UINT64_MAX - 1 - lane;
+            const uint64_t key = (c[0] | c[1] | c[2]) ? ctile : UINT64_MAX - 1 - lane;
             const uint32_t same = __match_any_sync(0xffffffffu, key);
-            const uint32_t s1 = __reduce_add_sync(same, c1), s2 = __reduce_add_sync(same, c2);
-            if (key == ctile && lane == (uint32_t)(__ffs(same) - 1)) {
-                const uint64_t slot = ctile - tile_base;
-                if (slot < a.tmax) {
-                    if (s1) atomicAdd(cnt_s + slot * stride + 1, s1);
-                    if (s2) atomicAdd(cnt_s + slot * stride + 2, s2);
-                } else if (ctile < a.ntiles) {
-                    if (s1) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 1], (unsigned long long)s1);
-                    if (s2) atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 2], (unsigned long long)s2);
+            const uint32_t leader = __ffs(same) - 1;
+#pragma unroll
+            for (int g = 0; g < 3; ++g) {
+                const uint32_t sum = __reduce_add_sync(same, c[g]);
+                if (key == ctile && lane == leader && sum) {
+                    const uint64_t slot = ctile - tile_base;
+                    if (slot < a.tmax) atomicAdd(cnt_s + slot * stride + 1 + g, sum);
+                    else if (ctile < a.ntiles)
+                        atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 1 + g], (unsigned long long)sum);
                 }
-            }
-            c1 = c2 = 0;
-        };
-
-        auto drain = [&](uint32_t n) {                    // exact later filters, one queued survivor per lane
-            __syncwarp();
-            const bool mine = lane < n;
-            uint64_t v = 0;
-            uint32_t meta = 0;
-            if (mine) {
-                v = qv[(qhead + lane) & (QCAP - 1)];
-                meta = qm[(qhead + lane) & (QCAP - 1)];
-            }
-            __syncwarp();
-            qhead += n;
-            bool pass = false;
-            u128 x{0, 0};
-            const uint32_t slot = meta >> 12;
-            const uint64_t tile = slot == SLOT_FAR ? tile_of(v, a.v_first, a.width) : tile_base + slot;
-            if (mine && tile < a.ntiles) {
-                uint32_t *cs = slot < a.tmax ? cnt_s + slot * stride : nullptr;
-                const u128 pos = mul_wide(us_s[meta & 0xfff], a.B), shift = mul_wide(v, a.A);
-                if (less128(pos, shift)) {
-                    atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 2], 1ull);
-                } else {
-                    x = sub128(pos, shift);
-                    const uint32_t h[6] = {(uint32_t)x.lo & 0xffffu, (uint32_t)(x.lo >> 16) & 0xffffu,
-                                           (uint32_t)(x.lo >> 32) & 0xffffu, (uint32_t)(x.lo >> 48),
-                                           (uint32_t)x.hi & 0xffffu, (uint32_t)(x.hi >> 16) & 0xffffu};
-                    pass = true;
-                    for (uint32_t idx = NB; idx < a.nres; ++idx) {
-                        const FiltC f = a.fcs[idx];
-                        const uint32_t m = mod_limbs(h, f);
-                        if (!((__ldg(a.bits + f.tab_off + (m >> 5)) >> (m & 31)) & 1u)) {
-                            pass = false;
-                            break;
-                        }
-                        if ((idx & 3) == 3 || idx + 1 == a.nres) {
-                            const uint32_t g = idx / 4 + 1;
-                            if (cs) atomicAdd(cs + g, 1u);
-                            else atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], 1ull);
-                        }
-                    }
-                    if (pass) {
-                        if (cs) atomicAdd(cs + a.ng + 1, 1u);
-                        else atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 1], 1ull);
-                    }
-                }
-            }
-            const uint32_t won = __ballot_sync(0xffffffffu, pass);
-            if (won) {
-                const uint32_t leader = __ffs(won) - 1;
-                unsigned long long first = 0;
-                if (lane == leader) first = atomicAdd(a.n_out, (unsigned long long)__popc(won));
-                first = __shfl_sync(0xffffffffu, first, leader);
-                if (pass) {
-                    const unsigned long long o = first + __popc(won & lanes_below);
-                    if (o < a.out_cap) {
-                        a.out[2 * o] = x.lo;
-                        a.out[2 * o + 1] = x.hi | (tile << 32);
-                    }
-                }
+                c[g] = 0;
             }
         };
 
@@ -507,8 +471,10 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             uint32_t ro[NB];                              // unit offset of each filter's row
 #pragma unroll
             for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)(active ? rec.row[f] : a.row0[f]) * U;
-            const uint64_t slot64 = ctile - tile_base;
-            const uint32_t meta_hi = (slot64 < SLOT_FAR ? (uint32_t)slot64 : SLOT_FAR) << 12;
+            uint32_t vr[PC_MAX_CHEAP];                    // v*A mod q of the cheap-tier filters
+#pragma unroll
+            for (int t = 0; t < PC_MAX_CHEAP; ++t)
+                vr[t] = t < (int)nch ? fastmod32(mod64(rec.v, a.cmq[t]) * a.caq[t], a.cmq[t].c, a.cq[t]) : 0u;
 
 #pragma unroll 1
             for (uint32_t p = 0; p < U; ++p) {
@@ -532,45 +498,128 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                     acc.x &= m0, acc.y &= m1, acc.z &= m2, acc.w &= m3;
                     acc4.x &= m0, acc4.y &= m1, acc4.z &= m2, acc4.w &= m3;
                 }
-                c1 += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
-                if (c2_live) c2 += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
-                while (__any_sync(0xffffffffu, (acc.x | acc.y | acc.z | acc.w) != 0)) {
-                    const bool has = (acc.x | acc.y | acc.z | acc.w) != 0;
-                    const uint32_t bal = __ballot_sync(0xffffffffu, has);
-                    if (has) {
-                        uint32_t bit;
-                        if (acc.x) {
-                            bit = __ffs(acc.x) - 1;
-                            acc.x &= acc.x - 1;
-                        } else if (acc.y) {
-                            bit = 32 + __ffs(acc.y) - 1;
-                            acc.y &= acc.y - 1;
-                        } else if (acc.z) {
-                            bit = 64 + __ffs(acc.z) - 1;
-                            acc.z &= acc.z - 1;
-                        } else {
-                            bit = 96 + __ffs(acc.w) - 1;
-                            acc.w &= acc.w - 1;
-                        }
-                        const uint32_t at = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
-                        qv[at] = rec.v;
-                        qm[at] = (u * 128 + bit) | meta_hi;
+                c[0] += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
+                if (c2_live) c[1] += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
+                while (acc.x | acc.y | acc.z | acc.w) {   // survivors of every bitset filter (rare)
+                    uint32_t bit;
+                    if (acc.x) {
+                        bit = __ffs(acc.x) - 1;
+                        acc.x &= acc.x - 1;
+                    } else if (acc.y) {
+                        bit = 32 + __ffs(acc.y) - 1;
+                        acc.y &= acc.y - 1;
+                    } else if (acc.z) {
+                        bit = 64 + __ffs(acc.z) - 1;
+                        acc.z &= acc.z - 1;
+                    } else {
+                        bit = 96 + __ffs(acc.w) - 1;
+                        acc.w &= acc.w - 1;
                     }
-                    qtail += __popc(bal);
-                    if (qtail - qhead >= 32) drain(32);
+                    const uint32_t uidx = u * 128 + bit;
+                    bool pass = true;
+#pragma unroll
+                    for (int t = 0; t < PC_MAX_CHEAP; ++t) {
+                        if (t < (int)nch && pass) {
+                            int32_t m = (int32_t)ures[t * G::UB + uidx] - (int32_t)vr[t];
+                            if (m < 0) m += (int32_t)a.cq[t];
+                            if ((cbits[t * CBW + (m >> 5)] >> (m & 31)) & 1u) {
+                                const uint32_t g = a.bgroup[NB + t];   // groups 2 or 3: the tier starts at filter 4 or later
+                                c[1] += g == 2;
+                                c[2] += g == 3;
+                            } else {
+                                pass = false;
+                            }
+                        }
+                    }
+                    if (pass) {
+                        const uint32_t at = atomicAdd(deep_ctr, 1u);
+                        if (at < a.deep_cap)
+                            deep_slice[at] = make_uint4((uint32_t)rec.v, (uint32_t)(rec.v >> 32), block_u0 + uidx,
+                                                        (uint32_t)ctile);
+                    }
                 }
             }
         }
-        if (qtail != qhead) drain(qtail - qhead);
         flush();
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) {
-            uint32_t c = cnt_s[k];
-            if (c) {
+            uint32_t cv = cnt_s[k];
+            if (cv) {
                 uint32_t slot = k / stride, g = k % stride;
                 uint64_t tile = tile_base + slot;
                 if (tile < a.ntiles)
-                    atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], (unsigned long long)c);
+                    atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], (unsigned long long)cv);
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) a.deep_count[blockIdx.x] = *deep_ctr;
+}
+
+// x mod q for x < 2^96 from its six 16-bit limbs h (h[0] + sum h[k] (2^16k mod q), then one
+// fast remainder; every partial sum stays below 2^32 because q < 2^13).
+__device__ __forceinline__ uint32_t mod_limbs(const uint32_t h[6], const FiltC &f) {
+    uint32_t t = h[0] + h[1] * f.r16[0] + h[2] * f.r16[1] + h[3] * f.r16[2] + h[4] * f.r16[3] + h[5] * f.r16[4];
+    return fastmod32(t, f.c, f.q);
+}
+
+// Exact later filters on every deep record: x = uB - vA in two 64-bit limbs, filters first..nres-1
+// with group counters, then the output record.  One record per thread; outputs are appended with
+// one atomic per warp.
+__global__ void __launch_bounds__(256) k_deep(const DeepArgs a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lanes_below = (1u << lane) - 1u;
+    const uint32_t slice = blockIdx.y;
+    const uint32_t count = min(a.deep_count[slice], a.deep_cap);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+        const uint32_t at = base + threadIdx.x;
+        const uint64_t i = (uint64_t)slice * a.deep_cap + at;
+        const bool mine = at < count;
+        bool pass = false;
+        u128 x{0, 0};
+        uint64_t tile = 0;
+        if (mine) {
+            const uint4 r = a.deep[i];
+            const uint64_t v = (uint64_t)r.y << 32 | r.x;
+            tile = r.w;
+            const u128 pos = mul_wide(__ldg(a.us + r.z), a.B), shift = mul_wide(v, a.A);
+            if (tile >= a.ntiles) {
+            } else if (less128(pos, shift)) {
+                atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 2], 1ull);
+            } else {
+                x = sub128(pos, shift);
+                const uint32_t h[6] = {(uint32_t)x.lo & 0xffffu, (uint32_t)(x.lo >> 16) & 0xffffu,
+                                       (uint32_t)(x.lo >> 32) & 0xffffu, (uint32_t)(x.lo >> 48),
+                                       (uint32_t)x.hi & 0xffffu, (uint32_t)(x.hi >> 16) & 0xffffu};
+                pass = true;
+                for (uint32_t idx = a.first; idx < a.nres; ++idx) {
+                    const FiltC f = a.fcs[idx];
+                    const uint32_t m = mod_limbs(h, f);
+                    if (!((__ldg(a.bits + f.tab_off + (m >> 5)) >> (m & 31)) & 1u)) {
+                        pass = false;
+                        break;
+                    }
+                    if ((idx & 3) == 3 || idx + 1 == a.nres)
+                        atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + idx / 4 + 1], 1ull);
+                }
+            }
+        }
+        const uint32_t won = __ballot_sync(0xffffffffu, pass);
+        if (won) {
+            const uint32_t leader = __ffs(won) - 1;
+            unsigned long long first = 0;
+            if (lane == leader) first = atomicAdd(a.n_out, (unsigned long long)__popc(won));
+            first = __shfl_sync(0xffffffffu, first, leader);
+            if (pass) {
+                const uint32_t same = __match_any_sync(won, tile);
+                if (lane == (uint32_t)(__ffs(same) - 1))
+                    atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 1],
+                              (unsigned long long)__popc(same));
+                const unsigned long long o = first + __popc(won & lanes_below);
+                if (o < a.out_cap) {
+                    a.out[2 * o] = x.lo;
+                    a.out[2 * o + 1] = x.hi | (tile << 32);
+                }
             }
         }
     }
@@ -778,9 +827,16 @@ extern "C" int pc_filters_free(pc_ctx *ctx, pc_filters *f) {
 namespace {
 
 struct Tuned {
-    uint32_t nb, K, threads;
+    uint32_t nb, K, threads, nch;
     uint64_t v_chunk;
 };
+
+// Residual filters after the bitset tier that the cheap tier can test (bitmap of <= 64 words).
+uint32_t cheap_count(const pc_filters *f, uint32_t nb) {
+    uint32_t n = 0;
+    while (n < PC_MAX_CHEAP && nb + n < f->nres && f->primes[nb + n] <= 2047) ++n;
+    return n;
+}
 
 Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_t *smem_out, uint32_t *tmax_out) {
     Tuned r{};
@@ -797,8 +853,9 @@ Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
     if (optin <= 0) optin = 227 * 1024;
     for (;;) {
+        r.nch = cheap_count(f, r.nb);
         for (uint32_t tmax = TMAX_DEFAULT; tmax >= 4; tmax /= 2) {
-            MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, tmax, f->ng, r.threads / 32);
+            MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, r.nch, tmax, f->ng);
             if (L.total <= (uint32_t)optin) {
                 *tmax_out = tmax;
                 *smem_out = L.total;
@@ -833,149 +890,205 @@ int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const 
     uint32_t tmax = 0;
     Tuned tn = resolve_tuning(ctx, f, tuning, &smem, &tmax);
     if (!smem) return pc_fail(ctx, PC_INVALID, "residual rows do not fit shared memory");
-    Scratch s(ctx);
-    uint64_t *d_counts, *d_geo, *d_out, *d_prefix, *d_vchunk, *d_pieces;
-    unsigned long long *d_nout, *d_bad;
-    VRec *d_rec;
-    uint4 *d_bv;
-    const uint32_t UB = tn.K * 32;
-    const uint64_t nblocks = (nu + UB - 1) / UB;
-    int rc = s.get(&d_counts, (uint64_t)ntiles * stride);
-    if (!rc) rc = s.get(&d_geo, 2 * (uint64_t)ntiles);
-    if (!rc) rc = s.get(&d_out, 2 * std::max<uint64_t>(1, io.out_cap));
-    if (!rc) rc = s.get(&d_nout, 2);
-    if (!rc) rc = s.get(&d_rec, std::max<uint64_t>(1, nv));
-    if (!rc) rc = s.get(&d_bv, std::max<uint64_t>(1, nblocks));
-    if (!rc) rc = s.get(&d_pieces, std::max<uint64_t>(1, nblocks));
-    if (!rc) rc = s.get(&d_prefix, nblocks + 1);
-    if (!rc) rc = s.get(&d_vchunk, 1);
-    if (rc) return rc;
-    d_bad = d_nout + 1;
-    cudaStream_t st = ctx->stream;
-    PC_CHECK(ctx, cudaMemsetAsync(d_counts, 0, (uint64_t)ntiles * stride * 8, st));
-    PC_CHECK(ctx, cudaMemsetAsync(d_nout, 0, 16, st));
-    PC_CHECK(ctx, cudaEventRecord(ctx->ev[0], st));
-    int launches = launches0;
+    const int grid = ctx->sm_count;
+    uint32_t deep_cap = 1u << 15;
+    for (int attempt = 0;; ++attempt) {
+        Scratch s(ctx);
+        uint64_t *d_counts, *d_geo, *d_out, *d_prefix, *d_vchunk, *d_pieces;
+        unsigned long long *d_nout, *d_bad;
+        VRec *d_rec;
+        uint4 *d_bv, *d_deep;
+        uint32_t *d_deep_count;
+        const uint32_t UB = tn.K * 32;
+        const uint64_t nblocks = (nu + UB - 1) / UB;
+        int rc = s.get(&d_counts, (uint64_t)ntiles * stride);
+        if (!rc) rc = s.get(&d_geo, 2 * (uint64_t)ntiles);
+        if (!rc) rc = s.get(&d_out, 2 * std::max<uint64_t>(1, io.out_cap));
+        if (!rc) rc = s.get(&d_nout, 2);
+        if (!rc) rc = s.get(&d_rec, std::max<uint64_t>(1, nv));
+        if (!rc) rc = s.get(&d_bv, std::max<uint64_t>(1, nblocks));
+        if (!rc) rc = s.get(&d_pieces, std::max<uint64_t>(1, nblocks));
+        if (!rc) rc = s.get(&d_prefix, nblocks + 1);
+        if (!rc) rc = s.get(&d_vchunk, 1);
+        if (!rc) rc = s.get(&d_deep, (uint64_t)grid * deep_cap);
+        if (!rc) rc = s.get(&d_deep_count, grid);
+        if (rc) return rc;
+        d_bad = d_nout + 1;
+        cudaStream_t st = ctx->stream;
+        PC_CHECK(ctx, cudaMemsetAsync(d_counts, 0, (uint64_t)ntiles * stride * 8, st));
+        PC_CHECK(ctx, cudaMemsetAsync(d_nout, 0, 16, st));
+        PC_CHECK(ctx, cudaMemsetAsync(d_deep_count, 0, (uint64_t)grid * 4, st));
+        PC_CHECK(ctx, cudaEventRecord(ctx->ev[0], st));
+        int launches = launches0;
 
-    PrepArgs pa{};
-    pa.us = d_us;
-    pa.vs = d_vs;
-    pa.nu = nu;
-    pa.nv = nv;
-    pa.A = f->A;
-    pa.B = f->B;
-    pa.lo = lo;
-    pa.hi = hi;
-    pa.v_first = v_first;
-    pa.width = width;
-    pa.ntiles = ntiles;
-    pa.nb = tn.nb;
-    pa.ng = ng;
-    for (uint32_t i = 0; i < tn.nb; ++i) {
-        pa.q[i] = f->primes[i];
-        pa.row0[i] = f->rows_sum[i];
-        pa.mq[i] = make_modq(f->primes[i]);
-    }
-    pa.rec = d_rec;
-    pa.counts = d_counts;
-    pa.bad = d_bad;
-    if (nv) {
-        uint64_t runs = (nv + PREP_RUN - 1) / PREP_RUN;
-        k_vprep<<<(unsigned)((runs + 127) / 128), 128, 0, st>>>(pa);
-        PC_LAUNCHED(ctx, "vprep");
-        ++launches;
-    }
-    k_geometry<<<(ntiles + 127) / 128, 128, 0, st>>>(d_us, nu, d_vs, nv, f->A, f->B, lo, hi, v_first, width, v_end,
-                                                      ntiles, d_geo);
-    PC_LAUNCHED(ctx, "geometry");
-    ++launches;
-    PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], st));
-    bool run_match = nu && nv;
-    if (run_match) {
-        k_blocks<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_rec, nv, nu, UB, nblocks, d_bv, d_pieces);
-        PC_LAUNCHED(ctx, "blocks");
-        int grid = ctx->sm_count;
-        uint64_t *d_items, *d_tmp;
-        rc = s.get(&d_items, nblocks);
-        if (!rc) rc = s.get(&d_tmp, nblocks + 1);
-        if (!rc) rc = pc_exclusive_scan_u64(ctx, d_pieces, d_tmp, nblocks, d_tmp + nblocks);
-        if (rc) return rc;
-        k_chunk<<<1, 1, 0, st>>>(d_tmp + nblocks, tn.v_chunk, (uint64_t)grid * 32, d_vchunk);
-        PC_LAUNCHED(ctx, "chunk");
-        k_item_counts<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_pieces, nblocks, d_vchunk, d_items);
-        PC_LAUNCHED(ctx, "item counts");
-        rc = pc_exclusive_scan_u64(ctx, d_items, d_prefix, nblocks, d_prefix + nblocks);
-        if (rc) return rc;
-        launches += 7;
-        MatchArgs ma{};
-        ma.us = d_us;
-        ma.vs = d_vs;
-        ma.rec = d_rec;
-        ma.nu = nu;
-        ma.nv = nv;
-        ma.A = f->A;
-        ma.B = f->B;
-        ma.lo = lo;
-        ma.hi = hi;
-        ma.nres = f->nres;
-        ma.ng = ng;
-        ma.nb = tn.nb;
-        ma.tmax = tmax;
-        ma.fc = f->d_fc;
-        ma.bits = f->d_bits;
-        ma.pat = f->d_pat;
+        PrepArgs pa{};
+        pa.us = d_us;
+        pa.vs = d_vs;
+        pa.nu = nu;
+        pa.nv = nv;
+        pa.A = f->A;
+        pa.B = f->B;
+        pa.lo = lo;
+        pa.hi = hi;
+        pa.v_first = v_first;
+        pa.width = width;
+        pa.ntiles = ntiles;
+        pa.nb = tn.nb;
+        pa.ng = ng;
         for (uint32_t i = 0; i < tn.nb; ++i) {
-            ma.q[i] = f->primes[i];
-            ma.row0[i] = f->rows_sum[i];
-            ma.ainvb[i] = f->ainvb[i];
-            ma.mq[i] = make_modq(f->primes[i]);
+            pa.q[i] = f->primes[i];
+            pa.row0[i] = f->rows_sum[i];
+            pa.mq[i] = make_modq(f->primes[i]);
         }
-        ma.total_rows = f->rows_sum[tn.nb];
-        ma.counts = d_counts;
-        ma.out = d_out;
-        ma.out_cap = io.out_cap;
-        ma.n_out = d_nout;
-        ma.ntiles = ntiles;
-        ma.bv = d_bv;
-        ma.item_prefix = d_prefix;
-        ma.nblocks = nblocks;
-        ma.vchunk = d_vchunk;
-        ma.v_first = v_first;
-        ma.width = width;
-        for (uint32_t i = 0; i < f->nres && i < (uint32_t)FC_INLINE; ++i) ma.fcs[i] = f->fcs[i];
-        PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
-        if (tn.threads == 1024) rc = launch_match_n<1024>(ctx, ma, tn.K, smem, grid);
-        else if (tn.threads == 768) rc = launch_match_n<768>(ctx, ma, tn.K, smem, grid);
-        else rc = launch_match_n<512>(ctx, ma, tn.K, smem, grid);
-        if (rc) return rc;
+        pa.rec = d_rec;
+        pa.counts = d_counts;
+        pa.bad = d_bad;
+        if (nv) {
+            uint64_t runs = (nv + PREP_RUN - 1) / PREP_RUN;
+            k_vprep<<<(unsigned)((runs + 127) / 128), 128, 0, st>>>(pa);
+            PC_LAUNCHED(ctx, "vprep");
+            ++launches;
+        }
+        k_geometry<<<(ntiles + 127) / 128, 128, 0, st>>>(d_us, nu, d_vs, nv, f->A, f->B, lo, hi, v_first, width,
+                                                          v_end, ntiles, d_geo);
+        PC_LAUNCHED(ctx, "geometry");
         ++launches;
-        PC_CHECK(ctx, cudaEventRecord(ctx->ev[3], st));
-    }
-    unsigned long long host_nout[2] = {0, 0};
-    PC_CHECK(ctx, cudaMemcpyAsync(host_nout, d_nout, 16, cudaMemcpyDeviceToHost, st));
-    PC_CHECK(ctx, cudaMemcpyAsync(io.counts, d_counts, (uint64_t)ntiles * stride * 8, cudaMemcpyDeviceToHost, st));
-    PC_CHECK(ctx, cudaMemcpyAsync(io.geometry, d_geo, 2 * (uint64_t)ntiles * 8, cudaMemcpyDeviceToHost, st));
-    PC_CHECK(ctx, cudaStreamSynchronize(st));
-    uint64_t n = host_nout[0];
-    *io.n_out = n;
-    if (io.stats) {
-        io.stats->bounds_ms = elapsed_ms(ctx->ev[0], ctx->ev[1]);
-        io.stats->kernel_ms = run_match ? elapsed_ms(ctx->ev[2], ctx->ev[3]) : 0.0;
-        io.stats->outputs = n;
-        io.stats->launches = launches;
-        io.stats->reserved[0] = tn.nb;
-        io.stats->reserved[1] = tn.K;
-        io.stats->reserved[2] = tn.threads;
-    }
-    if (host_nout[1]) return pc_fail(ctx, PC_INVALID, "v row outside the subtile geometry");
-    if (n > io.out_cap) return pc_fail(ctx, PC_OVERFLOW, "output overflow; attempt cannot commit");
-    if (n) {
-        PC_CHECK(ctx, cudaMemcpyAsync(io.out, d_out, 2 * n * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], st));
+        const bool run_match = nu && nv;
+        uint32_t deep_max = 0;
+        if (run_match) {
+            k_blocks<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_rec, nv, nu, UB, nblocks, d_bv, d_pieces);
+            PC_LAUNCHED(ctx, "blocks");
+            uint64_t *d_items, *d_tmp;
+            rc = s.get(&d_items, nblocks);
+            if (!rc) rc = s.get(&d_tmp, nblocks + 1);
+            if (!rc) rc = pc_exclusive_scan_u64(ctx, d_pieces, d_tmp, nblocks, d_tmp + nblocks);
+            if (rc) return rc;
+            k_chunk<<<1, 1, 0, st>>>(d_tmp + nblocks, tn.v_chunk, (uint64_t)grid * 32, d_vchunk);
+            PC_LAUNCHED(ctx, "chunk");
+            k_item_counts<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_pieces, nblocks, d_vchunk, d_items);
+            PC_LAUNCHED(ctx, "item counts");
+            rc = pc_exclusive_scan_u64(ctx, d_items, d_prefix, nblocks, d_prefix + nblocks);
+            if (rc) return rc;
+            launches += 7;
+            MatchArgs ma{};
+            ma.us = d_us;
+            ma.vs = d_vs;
+            ma.rec = d_rec;
+            ma.nu = nu;
+            ma.nv = nv;
+            ma.A = f->A;
+            ma.B = f->B;
+            ma.lo = lo;
+            ma.hi = hi;
+            ma.nres = f->nres;
+            ma.ng = ng;
+            ma.nb = tn.nb;
+            ma.tmax = tmax;
+            ma.fc = f->d_fc;
+            ma.bits = f->d_bits;
+            ma.pat = f->d_pat;
+            for (uint32_t i = 0; i < tn.nb; ++i) {
+                ma.q[i] = f->primes[i];
+                ma.row0[i] = f->rows_sum[i];
+                ma.ainvb[i] = f->ainvb[i];
+                ma.mq[i] = make_modq(f->primes[i]);
+            }
+            ma.total_rows = f->rows_sum[tn.nb];
+            ma.counts = d_counts;
+            ma.out = d_out;
+            ma.out_cap = io.out_cap;
+            ma.n_out = d_nout;
+            ma.ntiles = ntiles;
+            ma.bv = d_bv;
+            ma.item_prefix = d_prefix;
+            ma.nblocks = nblocks;
+            ma.vchunk = d_vchunk;
+            ma.v_first = v_first;
+            ma.width = width;
+            ma.nch = tn.nch;
+            for (uint32_t t = 0; t < tn.nch; ++t) {
+                const uint32_t q = f->primes[tn.nb + t];
+                ma.cq[t] = q;
+                ma.caq[t] = (uint32_t)(f->A % q);
+                ma.cbq[t] = (uint32_t)(f->B % q);
+                ma.cmq[t] = make_modq(q);
+                ma.cbits_off[t] = f->fcs[tn.nb + t].tab_off;
+            }
+            for (uint32_t idx = 0; idx < 16; ++idx)
+                ma.bgroup[idx] = (uint8_t)(idx < f->nres && ((idx & 3) == 3 || idx + 1 == f->nres) ? idx / 4 + 1 : 0);
+            ma.deep = d_deep;
+            ma.deep_cap = deep_cap;
+            ma.deep_count = d_deep_count;
+            PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
+            if (tn.threads == 1024) rc = launch_match_n<1024>(ctx, ma, tn.K, smem, grid);
+            else if (tn.threads == 768) rc = launch_match_n<768>(ctx, ma, tn.K, smem, grid);
+            else rc = launch_match_n<512>(ctx, ma, tn.K, smem, grid);
+            if (rc) return rc;
+            ++launches;
+            std::vector<uint32_t> deep_counts(grid);
+            PC_CHECK(ctx, cudaMemcpyAsync(deep_counts.data(), d_deep_count, (uint64_t)grid * 4, cudaMemcpyDeviceToHost, st));
+            PC_CHECK(ctx, cudaStreamSynchronize(st));
+            for (uint32_t c : deep_counts) deep_max = std::max(deep_max, c);
+            if (deep_max > deep_cap) {
+                if (attempt) return pc_fail(ctx, PC_ARITHMETIC, "deep survivor count changed between attempts");
+                deep_cap = deep_max + 1024;
+                continue;                                  // rerun with room for every deep survivor
+            }
+            DeepArgs da{};
+            da.us = d_us;
+            da.deep = d_deep;
+            da.deep_count = d_deep_count;
+            da.deep_cap = deep_cap;
+            da.slices = grid;
+            da.A = f->A;
+            da.B = f->B;
+            da.first = tn.nb + tn.nch;
+            da.nres = f->nres;
+            da.ng = ng;
+            da.ntiles = ntiles;
+            da.bits = f->d_bits;
+            da.counts = d_counts;
+            da.out = d_out;
+            da.out_cap = io.out_cap;
+            da.n_out = d_nout;
+            for (uint32_t i = 0; i < f->nres && i < (uint32_t)FC_INLINE; ++i) da.fcs[i] = f->fcs[i];
+            if (deep_max) {
+                dim3 dg((unsigned)std::min<uint64_t>((deep_max + 255) / 256, 64), (unsigned)grid);
+                k_deep<<<dg, 256, 0, st>>>(da);
+                PC_LAUNCHED(ctx, "deep");
+                ++launches;
+            }
+            PC_CHECK(ctx, cudaEventRecord(ctx->ev[3], st));
+        }
+        unsigned long long host_nout[2] = {0, 0};
+        PC_CHECK(ctx, cudaMemcpyAsync(host_nout, d_nout, 16, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, cudaMemcpyAsync(io.counts, d_counts, (uint64_t)ntiles * stride * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, cudaMemcpyAsync(io.geometry, d_geo, 2 * (uint64_t)ntiles * 8, cudaMemcpyDeviceToHost, st));
         PC_CHECK(ctx, cudaStreamSynchronize(st));
+        uint64_t n = host_nout[0];
+        *io.n_out = n;
+        if (io.stats) {
+            io.stats->bounds_ms = elapsed_ms(ctx->ev[0], ctx->ev[1]);
+            io.stats->kernel_ms = run_match ? elapsed_ms(ctx->ev[2], ctx->ev[3]) : 0.0;
+            io.stats->outputs = n;
+            io.stats->launches = launches;
+            io.stats->work_items = deep_max;
+            io.stats->reserved[0] = tn.nb;
+            io.stats->reserved[1] = tn.K;
+            io.stats->reserved[2] = tn.threads;
+            io.stats->reserved[3] = tn.nch;
+        }
+        if (host_nout[1]) return pc_fail(ctx, PC_INVALID, "v row outside the subtile geometry");
+        if (n > io.out_cap) return pc_fail(ctx, PC_OVERFLOW, "output overflow; attempt cannot commit");
+        if (n) {
+            PC_CHECK(ctx, cudaMemcpyAsync(io.out, d_out, 2 * n * 8, cudaMemcpyDeviceToHost, st));
+            PC_CHECK(ctx, cudaStreamSynchronize(st));
+        }
+        for (uint32_t t = 0; t < ntiles; ++t)
+            if (io.counts[(uint64_t)t * stride + ng + 2]) return pc_fail(ctx, PC_ARITHMETIC, "unsigned underflow flagged");
+        return PC_OK;
     }
-    for (uint32_t t = 0; t < ntiles; ++t)
-        if (io.counts[(uint64_t)t * stride + ng + 2]) return pc_fail(ctx, PC_ARITHMETIC, "unsigned underflow flagged");
-    return PC_OK;
 }
 
 }  // namespace
