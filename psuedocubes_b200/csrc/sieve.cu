@@ -341,14 +341,23 @@ __device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, uint16_
 constexpr int CBW = 64;   // bitmap words per cheap-tier filter (q <= 2047)
 
 // Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.
+constexpr int QCAP = 64;              // survivor ring per warp (pending < 64 by construction)
+constexpr uint32_t SLOT_FAR = 0xFFFFF;  // queued slot too large to encode: the drain recomputes it
+
+// Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.  The
+// residue-row patterns are only read while rows are built, when every survivor ring is empty,
+// so they share the rings' space.
 struct MatchSmem {
-    uint32_t rows, ures, pat, cbits, cnt, misc, total;
+    uint32_t rows, ures, qv, qm, pat, cbits, cnt, misc, total;
     __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t nch, uint32_t tmax,
-                                  uint32_t ng) {
+                                  uint32_t ng, uint32_t warps) {
         rows = 0;
         ures = rows + total_rows * (K / 4) * 16;
-        pat = ures + ((nch * K * 32 * 2 + 15) & ~15u);
-        cbits = pat + nb * PATW * 4;
+        qv = ures + ((nch * K * 32 * 2 + 15) & ~15u);
+        qm = qv + warps * QCAP * 8;
+        pat = qv;
+        const uint32_t ring_end = qm + warps * QCAP * 4, pat_end = pat + nb * PATW * 4;
+        cbits = ((ring_end > pat_end ? ring_end : pat_end) + 15) & ~15u;
         cnt = cbits + nch * CBW * 4;
         misc = cnt + ((tmax * (ng + 2) * 4 + 15) & ~15u);
         total = misc + 16;
@@ -369,17 +378,19 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     constexpr uint32_t U = G::U;
     extern __shared__ uint4 smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const MatchSmem L(a.total_rows, K, NB, a.nch, a.tmax, a.ng);
+    const MatchSmem L(a.total_rows, K, NB, a.nch, a.tmax, a.ng, nwarps);
     char *base = (char *)smem;
     const uint4 *rows = (const uint4 *)(base + L.rows);
     uint16_t *ures = (uint16_t *)(base + L.ures);
+    uint64_t *qv = (uint64_t *)(base + L.qv) + warp * QCAP;
+    uint32_t *qm = (uint32_t *)(base + L.qm) + warp * QCAP;
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
     uint32_t *cbits = (uint32_t *)(base + L.cbits);
     uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ng+2): groups 1..ng, outputs
     uint32_t *deep_ctr = (uint32_t *)(base + L.misc);
     const uint32_t stride = a.ng + 2;
 
-    for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = a.pat[i];
+    const uint32_t lanes_below = (1u << lane) - 1u;
     for (uint32_t i = threadIdx.x; i < a.nch * CBW; i += blockDim.x) {
         const uint32_t t = i / CBW, w = i % CBW;
         cbits[i] = w * 32 < a.cq[t] ? a.bits[a.cbits_off[t] + w] : 0u;
@@ -415,6 +426,8 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         const uint32_t block_u0 = (uint32_t)(b * G::UB);
         __syncthreads();                                  // previous item finished with shared memory
         if (b != cur) {
+            for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = a.pat[i];
+            __syncthreads();
             build_rows<NB, K>(a, (uint4 *)rows, ures, pat_s, block_u0, lane, warp, nwarps);
             cur = b;
         }
@@ -440,6 +453,41 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                 }
                 c[g] = 0;
             }
+        };
+
+        uint32_t qhead = 0, qtail = 0;                    // warp-uniform ring positions
+
+        // Cheap-tier filters on up to 32 queued survivors, one per lane; survivors of all of them
+        // go to this CTA's deep slice.
+        auto drain = [&](uint32_t n) {
+            __syncwarp();
+            const bool mine = lane < n;
+            uint64_t v = 0;
+            uint32_t meta = 0;
+            if (mine) {
+                v = qv[(qhead + lane) & (QCAP - 1)];
+                meta = qm[(qhead + lane) & (QCAP - 1)];
+            }
+            __syncwarp();
+            qhead += n;
+            if (!mine) return;
+            const uint32_t uidx = meta & 0xfff, slot = meta >> 12;
+            const uint64_t tile = slot == SLOT_FAR ? tile_of(v, a.v_first, a.width) : tile_base + slot;
+            for (uint32_t t = 0; t < nch; ++t) {
+                const uint32_t vr = fastmod32(mod64(v, a.cmq[t]) * a.caq[t], a.cmq[t].c, a.cq[t]);
+                int32_t m = (int32_t)ures[t * G::UB + uidx] - (int32_t)vr;
+                if (m < 0) m += (int32_t)a.cq[t];
+                if (!((cbits[t * CBW + (m >> 5)] >> (m & 31)) & 1u)) return;
+                const uint32_t g = a.bgroup[NB + t];
+                if (g) {
+                    if (slot < a.tmax) atomicAdd(cnt_s + slot * stride + g, 1u);
+                    else if (tile < a.ntiles)
+                        atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], 1ull);
+                }
+            }
+            const uint32_t at = atomicAdd(deep_ctr, 1u);
+            if (at < a.deep_cap)
+                deep_slice[at] = make_uint4((uint32_t)v, (uint32_t)(v >> 32), block_u0 + uidx, (uint32_t)tile);
         };
 
         const uint32_t nrounds = (nv_item + 31) / 32;
@@ -471,10 +519,8 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             uint32_t ro[NB];                              // unit offset of each filter's row
 #pragma unroll
             for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)(active ? rec.row[f] : a.row0[f]) * U;
-            uint32_t vr[PC_MAX_CHEAP];                    // v*A mod q of the cheap-tier filters
-#pragma unroll
-            for (int t = 0; t < PC_MAX_CHEAP; ++t)
-                vr[t] = t < (int)nch ? fastmod32(mod64(rec.v, a.cmq[t]) * a.caq[t], a.cmq[t].c, a.cq[t]) : 0u;
+            const uint64_t slot64 = ctile - tile_base;
+            const uint32_t meta_hi = (slot64 < SLOT_FAR ? (uint32_t)slot64 : SLOT_FAR) << 12;
 
 #pragma unroll 1
             for (uint32_t p = 0; p < U; ++p) {
@@ -500,46 +546,34 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                 }
                 c[0] += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
                 if (c2_live) c[1] += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
-                while (acc.x | acc.y | acc.z | acc.w) {   // survivors of every bitset filter (rare)
-                    uint32_t bit;
-                    if (acc.x) {
-                        bit = __ffs(acc.x) - 1;
-                        acc.x &= acc.x - 1;
-                    } else if (acc.y) {
-                        bit = 32 + __ffs(acc.y) - 1;
-                        acc.y &= acc.y - 1;
-                    } else if (acc.z) {
-                        bit = 64 + __ffs(acc.z) - 1;
-                        acc.z &= acc.z - 1;
-                    } else {
-                        bit = 96 + __ffs(acc.w) - 1;
-                        acc.w &= acc.w - 1;
-                    }
-                    const uint32_t uidx = u * 128 + bit;
-                    bool pass = true;
-#pragma unroll
-                    for (int t = 0; t < PC_MAX_CHEAP; ++t) {
-                        if (t < (int)nch && pass) {
-                            int32_t m = (int32_t)ures[t * G::UB + uidx] - (int32_t)vr[t];
-                            if (m < 0) m += (int32_t)a.cq[t];
-                            if ((cbits[t * CBW + (m >> 5)] >> (m & 31)) & 1u) {
-                                const uint32_t g = a.bgroup[NB + t];   // groups 2 or 3: the tier starts at filter 4 or later
-                                c[1] += g == 2;
-                                c[2] += g == 3;
-                            } else {
-                                pass = false;
-                            }
+                while (__any_sync(0xffffffffu, (acc.x | acc.y | acc.z | acc.w) != 0)) {
+                    const bool has = (acc.x | acc.y | acc.z | acc.w) != 0;
+                    const uint32_t bal = __ballot_sync(0xffffffffu, has);
+                    if (has) {
+                        uint32_t bit;
+                        if (acc.x) {
+                            bit = __ffs(acc.x) - 1;
+                            acc.x &= acc.x - 1;
+                        } else if (acc.y) {
+                            bit = 32 + __ffs(acc.y) - 1;
+                            acc.y &= acc.y - 1;
+                        } else if (acc.z) {
+                            bit = 64 + __ffs(acc.z) - 1;
+                            acc.z &= acc.z - 1;
+                        } else {
+                            bit = 96 + __ffs(acc.w) - 1;
+                            acc.w &= acc.w - 1;
                         }
+                        const uint32_t at = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
+                        qv[at] = rec.v;
+                        qm[at] = (u * 128 + bit) | meta_hi;
                     }
-                    if (pass) {
-                        const uint32_t at = atomicAdd(deep_ctr, 1u);
-                        if (at < a.deep_cap)
-                            deep_slice[at] = make_uint4((uint32_t)rec.v, (uint32_t)(rec.v >> 32), block_u0 + uidx,
-                                                        (uint32_t)ctile);
-                    }
+                    qtail += __popc(bal);
+                    if (qtail - qhead >= 32) drain(32);
                 }
             }
         }
+        if (qtail != qhead) drain(qtail - qhead);
         flush();
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) {
@@ -855,7 +889,7 @@ Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_
     for (;;) {
         r.nch = cheap_count(f, r.nb);
         for (uint32_t tmax = TMAX_DEFAULT; tmax >= 4; tmax /= 2) {
-            MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, r.nch, tmax, f->ng);
+            MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, r.nch, tmax, f->ng, r.threads / 32);
             if (L.total <= (uint32_t)optin) {
                 *tmax_out = tmax;
                 *smem_out = L.total;
