@@ -141,38 +141,50 @@ __device__ __forceinline__ void unit_of(const WindowPlan &p, uint64_t words1, ui
     wb = min(p.wb1, wa + WIN_WORDS);
 }
 
+// One warp per window unit of WIN_WORDS = 32 wheel words, one word per lane, so every row load
+// of the warp is one coalesced 128-byte request.  Count pass: per-unit totals.  Emit pass: the
+// lane's exclusive prefix inside the warp plus the unit's offset gives ascending output slots.
 __global__ void k_window(const WindowArgs a, const uint64_t *__restrict__ W1, const uint32_t *__restrict__ rows,
                          uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
                          uint64_t *__restrict__ out) {
-    uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (u >= a.plan.units) return;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t u = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    if (u >= a.plan.units) return;                      // warp-uniform
     uint64_t K, wa, wb;
     unit_of(a.plan, a.words1, u, K, wa, wb);
-    const uint32_t *r[PC_MAX_WHEEL_T];
-    for (uint32_t t = 0; t < a.nT; ++t) {
-        uint32_t s = (uint32_t)(((uint64_t)mod64(K, a.tmq[t]) * a.t_m1mod[t]) % a.tq[t]);
-        r[t] = rows + (uint64_t)(a.t_row0[t] + s) * a.words1;
-    }
-    uint64_t jmin = K == a.plan.K0 ? a.plan.j_lo : 0;
-    uint64_t jmax = K == a.plan.K1 ? a.plan.j_hi : a.count1;
-    uint64_t base = K * a.M1, total = 0, pos = offsets ? offsets[u] : 0;
-    for (uint64_t w = wa; w < wb; ++w) {
-        uint32_t bits = 0xffffffffu;
-        for (uint32_t t = 0; t < a.nT; ++t) bits &= __ldg(r[t] + w);
-        uint64_t j0 = w * 32;
+    const uint64_t w = wa + lane;
+    uint32_t bits = 0;
+    if (w < wb) {
+        bits = 0xffffffffu;
+        for (uint32_t t = 0; t < a.nT; ++t) {
+            const uint32_t s = (uint32_t)(((uint64_t)mod64(K, a.tmq[t]) * a.t_m1mod[t]) % a.tq[t]);
+            bits &= __ldg(rows + (uint64_t)(a.t_row0[t] + s) * a.words1 + w);
+        }
+        const uint64_t jmin = K == a.plan.K0 ? a.plan.j_lo : 0;
+        const uint64_t jmax = K == a.plan.K1 ? a.plan.j_hi : a.count1;
+        const uint64_t j0 = w * 32;
         if (j0 < jmin) bits &= ~low_bits((uint32_t)(jmin - j0 < 32 ? jmin - j0 : 32));
         if (j0 + 32 > jmax) bits &= jmax > j0 ? low_bits((uint32_t)(jmax - j0)) : 0u;
-        if (offsets) {
-            while (bits) {
-                uint32_t b = __ffs(bits) - 1;
-                bits &= bits - 1;
-                out[pos++] = base + __ldg(W1 + j0 + b);
-            }
-        } else {
-            total += __popc(bits);
-        }
     }
-    if (!offsets) counts[u] = total;
+    const uint32_t n = __popc(bits);
+    if (!offsets) {
+        const uint32_t total = __reduce_add_sync(0xffffffffu, n);
+        if (lane == 0) counts[u] = total;
+        return;
+    }
+    uint32_t incl = n;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= (uint32_t)d) incl += y;
+    }
+    uint64_t pos = offsets[u] + incl - n;
+    const uint64_t base = K * a.M1, j0 = w * 32;
+    while (bits) {
+        const uint32_t b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        out[pos++] = base + __ldg(W1 + j0 + b);
+    }
 }
 
 // 128-bit product of 64-bit counts, host side.
@@ -443,7 +455,7 @@ int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, 
     if (!rc) rc = s.get(&d_off, p.units);
     if (!rc) rc = s.get(&d_total, 1);
     if (rc) return rc;
-    unsigned grid = (unsigned)((p.units + WT - 1) / WT);
+    unsigned grid = (unsigned)((p.units * 32 + WT - 1) / WT);
     k_window<<<grid, WT, 0, ctx->stream>>>(a, f->W1, f->rows, d_cnt, nullptr, nullptr);
     PC_LAUNCHED(ctx, "window count");
     rc = pc_exclusive_scan_u64(ctx, d_cnt, d_off, p.units, d_total);
