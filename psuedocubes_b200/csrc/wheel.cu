@@ -157,7 +157,7 @@ __global__ void k_window(const WindowArgs a, const uint64_t *__restrict__ W1, co
     if (w < wb) {
         bits = 0xffffffffu;
         for (uint32_t t = 0; t < a.nT; ++t) {
-            const uint32_t s = (uint32_t)(((uint64_t)mod64(K, a.tmq[t]) * a.t_m1mod[t]) % a.tq[t]);
+            const uint32_t s = fastmod32(mod64(K, a.tmq[t]) * a.t_m1mod[t], a.tmq[t].c, a.tq[t]);   // < q^2 < 2^32
             bits &= __ldg(rows + (uint64_t)(a.t_row0[t] + s) * a.words1 + w);
         }
         const uint64_t jmin = K == a.plan.K0 ? a.plan.j_lo : 0;
