@@ -141,6 +141,25 @@ int pc_run_plain(pc_ctx *ctx, const pc_filters *filters, const pc_buf *us, uint6
                  const pc_buf *vs, uint64_t v_off, uint64_t nv, uint64_t lo0, uint64_t lo1, uint64_t hi0,
                  uint64_t hi1, uint64_t *counts, uint64_t *out, uint64_t out_cap, pc_stats *stats);
 
+/*
+ * Plain per-tile matcher that allocates no device memory (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc: code that runs while a stream is being captured into
+ * a CUDA graph (allocation is refused there), code embedded in a process whose allocator already
+ * owns the device's memory, and code that must not pay cudaMalloc's implicit device
+ * synchronisation.  Same result as pc_run_plain with host inputs: us[nu], vs[nv] (sorted focus
+ * values of one tile), the residual filters as for pc_filters_create, counts [ng+3] and
+ * out [out_cap x 2] on the host.  Its scratch is a 16 MiB static device array inside the
+ * library: inputs, filter tables and outputs must fit in it, or the call returns PC_INVALID with
+ * the reason in err.  The first call on a device looks up the array's address (make that first
+ * call before any stream capture).  It works on the legacy default stream; every call reuses the
+ * same array, so calls that overlap on one GPU race with each other.  err (err_len bytes, may be
+ * NULL) receives a message on failure.
+ */
+int pc_run_plain_static(int device, const uint64_t *us, uint64_t nu, const uint64_t *vs, uint64_t nv,
+                        uint64_t A, uint64_t B, uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1,
+                        const uint32_t *primes, uint32_t nres, const uint8_t *allowed, uint64_t *counts,
+                        uint64_t *out, uint64_t out_cap, char *err, int err_len);
+
 /* 128-bit limb self-test: for each of n cases (a, b, c, d) in in4, out3 = low, high limb of
  * a*b - c*d mod 2^128 and the borrow flag; replaces the `arithmetic` kernel
  * (kernels/pseudocube.cuh:7-11). */

@@ -25,7 +25,7 @@ SYMBOLS = ('pc_version', 'pc_device_count', 'pc_last_error', 'pc_init', 'pc_free
            'pc_device_info', 'pc_sync', 'pc_mark', 'pc_elapsed', 'pc_buf_upload', 'pc_buf_download', 'pc_buf_size', 'pc_buf_free',
            'pc_buf_searchsorted', 'pc_focus_create', 'pc_focus_free', 'pc_focus_info', 'pc_focus_window',
            'pc_filters_create', 'pc_filters_free', 'pc_run_batch', 'pc_run_lease', 'pc_run_plain',
-           'pc_selftest_wide')
+           'pc_run_plain_static', 'pc_selftest_wide')
 
 
 class Tuning(ctypes.Structure):
@@ -92,6 +92,8 @@ def lib() -> ctypes.CDLL:
                                 ctypes.POINTER(Stats)]
     so.pc_run_plain.argtypes = [_P, _P, _P, _U64, _U64, _P, _U64, _U64, _U64, _U64, _U64, _U64,
                                 _U64P, _U64P, _U64, ctypes.POINTER(Stats)]
+    so.pc_run_plain_static.argtypes = [ctypes.c_int, _U64P, _U64, _U64P, _U64, _U64, _U64, _U64, _U64, _U64, _U64,
+                                       _U32P, _U32, _U8P, _U64P, _U64P, _U64, ctypes.c_char_p, ctypes.c_int]
     so.pc_selftest_wide.argtypes = [_P, _U64P, _U64P, _U64]
     return so
 

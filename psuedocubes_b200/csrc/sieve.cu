@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <cstdio>
 
 struct FiltConst {
     ModQ m;
@@ -1231,6 +1232,152 @@ extern "C" int pc_run_plain(pc_ctx *ctx, const pc_filters *f, const pc_buf *us, 
     if (copy) {
         PC_CHECK(ctx, cudaMemcpyAsync(out, d_out, 2 * copy * 8, cudaMemcpyDeviceToHost, st));
         PC_CHECK(ctx, cudaStreamSynchronize(st));
+    }
+    return PC_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Plain per-tile matcher with no device allocation (pc_run_plain_static).
+//
+// Its scratch is this file-scope device array, reserved when the library loads and held by every
+// GPU that loads it until the process exits.  Host code must not pass the array's name to a
+// kernel (on the host the name is only a stand-in, not a device address): the device address is
+// looked up once per device with cudaGetSymbolAddress and cached.  Every call reuses the same
+// bytes, so calls that overlap on one GPU race with each other.
+
+constexpr uint64_t STATIC_SCRATCH_BYTES = UINT64_C(16) << 20;   // 16 MiB
+static __device__ __align__(256) unsigned char g_static_scratch[STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr int STATIC_MAX_DEVICES = 64;
+unsigned char *g_static_ptr[STATIC_MAX_DEVICES] = {};
+
+inline uint64_t align256(uint64_t x) { return (x + 255) & ~UINT64_C(255); }
+
+int static_fail(char *err, int err_len, int code, const char *msg) {
+    if (err && err_len > 0) {
+        strncpy(err, msg, (size_t)err_len - 1);
+        err[err_len - 1] = 0;
+    }
+    return code;
+}
+
+int static_cuda(char *err, int err_len, cudaError_t e, const char *what) {
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    return static_fail(err, err_len, PC_CUDA, buf);
+}
+}  // namespace
+
+extern "C" int pc_run_plain_static(int device, const uint64_t *us, uint64_t nu, const uint64_t *vs, uint64_t nv,
+                                   uint64_t A, uint64_t B, uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1,
+                                   const uint32_t *primes, uint32_t nres, const uint8_t *allowed, uint64_t *counts,
+                                   uint64_t *out, uint64_t out_cap, char *err, int err_len) {
+    if (device < 0 || device >= STATIC_MAX_DEVICES) return static_fail(err, err_len, PC_INVALID, "device index out of range");
+    if (nres == 0 || nres > PC_MAX_RES || A == 0 || B == 0 || !counts || (nu && !us) || (nv && !vs))
+        return static_fail(err, err_len, PC_INVALID, "invalid plain tile arguments");
+    uint64_t words = 0;
+    for (uint32_t i = 0; i < nres; ++i) {
+        const uint32_t q = primes[i];
+        if (q < 2 || q >= 8192 || A % q == 0 || B % q == 0)
+            return static_fail(err, err_len, PC_INVALID, "residual modulus must be in [2, 8192) and coprime to A and B");
+        words += (q + 31) / 32;
+    }
+    const uint32_t ng = (nres + 3) / 4;
+    // layout of the static scratch: counters | filter constants | bitmaps | us | vs | outputs
+    const uint64_t o_counts = 0, o_fc = align256(o_counts + (ng + 3) * 8), o_bits = align256(o_fc + nres * sizeof(FiltConst));
+    const uint64_t o_us = align256(o_bits + words * 4), o_vs = align256(o_us + nu * 8), o_out = align256(o_vs + nv * 8);
+    const uint64_t need = o_out + 2 * (out_cap ? out_cap : 1) * 8;
+    if (need > STATIC_SCRATCH_BYTES)
+        return static_fail(err, err_len, PC_INVALID, "tile exceeds the 16 MiB static scratch of pc_run_plain_static");
+
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return static_cuda(err, err_len, e, "cudaSetDevice");
+    if (!g_static_ptr[device]) {          // set-up, once per device, with that device current
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess) return static_cuda(err, err_len, e, "cudaGetSymbolAddress");
+        g_static_ptr[device] = (unsigned char *)ptr;
+    }
+    unsigned char *base = g_static_ptr[device];
+    cudaStream_t st = 0;
+    // filter constants and packed bitmaps, staged through fixed host buffers
+    {
+        FiltConst fc[32];
+        uint32_t bits[1024];
+        uint64_t word_at = 0, nbits = 0, off = 0;
+        uint32_t nfc = 0, fc_at = 0;
+        for (uint32_t i = 0; i < nres; ++i) {
+            const uint32_t q = primes[i];
+            FiltConst &c = fc[nfc++];
+            c.m = make_modq(q);
+            c.tab_off = (uint32_t)(word_at + nbits);
+            c.pad = 0;
+            for (uint32_t w = 0; w < (q + 31) / 32; ++w) {
+                uint32_t v = 0;
+                for (uint32_t r = w * 32; r < q && r < w * 32 + 32; ++r)
+                    if (allowed[off + r]) v |= 1u << (r - w * 32);
+                bits[nbits++] = v;
+                if (nbits == 1024) {
+                    e = cudaMemcpyAsync(base + o_bits + word_at * 4, bits, nbits * 4, cudaMemcpyHostToDevice, st);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                    if (e != cudaSuccess) return static_cuda(err, err_len, e, "bitmap upload");
+                    word_at += nbits;
+                    nbits = 0;
+                }
+            }
+            off += q;
+            if (nfc == 32 || i + 1 == nres) {
+                e = cudaMemcpyAsync(base + o_fc + (uint64_t)fc_at * sizeof(FiltConst), fc, nfc * sizeof(FiltConst),
+                                    cudaMemcpyHostToDevice, st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess) return static_cuda(err, err_len, e, "filter upload");
+                fc_at += nfc;
+                nfc = 0;
+            }
+        }
+        if (nbits) {
+            e = cudaMemcpyAsync(base + o_bits + word_at * 4, bits, nbits * 4, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return static_cuda(err, err_len, e, "bitmap upload");
+        }
+    }
+    e = cudaMemsetAsync(base + o_counts, 0, (ng + 3) * 8, st);   // the array keeps the previous call's counts
+    if (e == cudaSuccess && nu) e = cudaMemcpyAsync(base + o_us, us, nu * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nv) e = cudaMemcpyAsync(base + o_vs, vs, nv * 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return static_cuda(err, err_len, e, "input upload");
+    if (nu && nv) {
+        int sm = 0;
+        cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device);
+        PlainArgs a{};
+        a.us = (const uint64_t *)(base + o_us);
+        a.vs = (const uint64_t *)(base + o_vs);
+        a.nu = nu;
+        a.nv = nv;
+        a.A = A;
+        a.B = B;
+        a.lo = u128{lo0, lo1};
+        a.hi = u128{hi0, hi1};
+        a.nres = nres;
+        a.ng = ng;
+        a.fc = (const FiltConst *)(base + o_fc);
+        a.bits = (const uint32_t *)(base + o_bits);
+        a.counts = (uint64_t *)(base + o_counts);
+        a.out = (uint64_t *)(base + o_out);
+        a.out_cap = out_cap;
+        uint64_t blocks = std::min<uint64_t>((nv + 7) / 8, (uint64_t)std::max(sm, 1) * 8);
+        k_plain<<<(unsigned)blocks, 256, 0, st>>>(a);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return static_cuda(err, err_len, e, "plain match launch");
+    }
+    e = cudaMemcpyAsync(counts, base + o_counts, (ng + 3) * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return static_cuda(err, err_len, e, "counter download");
+    const uint64_t copy = std::min(counts[ng + 1], out_cap);
+    if (copy && out) {
+        e = cudaMemcpyAsync(out, base + o_out, 2 * copy * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return static_cuda(err, err_len, e, "output download");
     }
     return PC_OK;
 }
