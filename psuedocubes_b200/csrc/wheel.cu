@@ -130,8 +130,10 @@ __device__ __forceinline__ void unit_of(const WindowPlan &p, uint64_t words1, ui
     u -= p.units_first;
     uint64_t mid_periods = p.K1 > p.K0 + 1 ? p.K1 - p.K0 - 1 : 0;
     if (u < mid_periods * p.units_mid) {
-        K = p.K0 + 1 + u / p.units_mid;
-        wa = (u % p.units_mid) * WIN_WORDS;
+        const uint32_t um = (uint32_t)p.units_mid, uu = (uint32_t)u;     // unit counts < 2^32
+        const uint32_t period = uu / um;
+        K = p.K0 + 1 + period;
+        wa = (uint64_t)(uu - period * um) * WIN_WORDS;
         wb = min(words1, wa + WIN_WORDS);
         return;
     }
@@ -449,6 +451,7 @@ int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, 
     uint64_t mid_periods = p.K1 > p.K0 + 1 ? p.K1 - p.K0 - 1 : 0;
     p.units = p.units_first + mid_periods * p.units_mid + p.units_last;
     if (p.units == 0) return PC_OK;
+    if (p.units >= (UINT64_C(1) << 31)) return pc_fail(ctx, PC_OVERFLOW, "focus window too long");
     Scratch s(ctx);
     uint64_t *d_cnt, *d_off, *d_total;
     int rc = s.get(&d_cnt, p.units);
