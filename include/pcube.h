@@ -85,10 +85,12 @@ int pc_filters_free(pc_ctx *ctx, pc_filters *filters);
 typedef struct pc_tuning {
     uint32_t bitset_filters;   /* residual filters intersected as bitsets (1..8, >= min(4, nres)) */
     uint32_t block_words;      /* u words (32 u each) staged per CTA: 16, 32 or 64 */
-    uint32_t words_per_thread; /* bitset words per thread per v row: 1, 2 or 4 */
-    uint32_t v_chunk;          /* v rows per work item (0 = whole block) */
-    uint32_t threads;          /* threads per CTA: 256, 512 or 1024 */
-    uint32_t reserved[3];
+    uint32_t words_per_thread; /* ignored: a lane walks all block_words words of its (v row, block) piece */
+    uint32_t v_chunk;          /* v rows per work item (0 = total pieces / (32 x SMs), at least 64) */
+    uint32_t threads;          /* threads per CTA: 512, 768 or 1024 */
+    uint32_t deep_records;     /* survivor buffer: deep records per CTA slice (0 = 32768); a run that
+                                  needs more reruns once with room for every record */
+    uint32_t reserved[2];
 } pc_tuning;
 
 /* Per-call statistics. */
@@ -100,7 +102,8 @@ typedef struct pc_stats {
     uint64_t work_items;
     uint64_t outputs;
     uint64_t launches;         /* kernels launched by the call */
-    uint64_t reserved[5];      /* [0..2]: bitset filters, block words and threads the call used */
+    uint64_t reserved[5];      /* [0..3]: bitset filters, block words, threads and cheap-tier
+                                  filters the call used; [4]: 1 when a recorded graph ran */
 } pc_stats;
 
 /*
@@ -132,6 +135,47 @@ int pc_run_lease(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb, const pc_f
                  uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1,
                  uint64_t *counts, uint64_t *geometry, uint64_t *out, uint64_t out_cap, uint64_t *n_out,
                  pc_stats *stats);
+
+/* Flags of pc_multi_run. */
+#define PC_RUN_GRAPH 1u   /* record the run into a CUDA graph once, then replay it on every call */
+
+/* One window of a multi-window launch. */
+typedef struct pc_window {
+    uint64_t first, end;          /* canonical v range [first, end) */
+    uint64_t width;               /* subtile width in v */
+    uint64_t lo0, lo1, hi0, hi1;  /* interval (lo, hi] as two limbs each, hi < 2^96 */
+    uint32_t focus_a, focus_b;    /* indices into the focus array (moduli A and B of the family) */
+    uint32_t family;              /* index into the filter-family array */
+    uint32_t reserved;
+} pc_window;
+
+typedef struct pc_multi pc_multi;   /* planned multi-window launch with its device buffers */
+
+/*
+ * Many windows in one launch sequence, each with its own interval, v range, subtile width, focus
+ * pair and filter family (prime bound): the batched form of compute_lease and of Matcher.tile
+ * over many tiles (pseudocube/optimized.py:81-90, pseudocube/gpu.py:212-234), for which the
+ * reference has no single call.  pc_multi_create plans the u and v windows of every window and
+ * sizes every device buffer (out_cap output records in all); pc_multi_run regenerates the windows
+ * on the device and runs stages 2 and 3 over all of them.  With PC_RUN_GRAPH the first call runs
+ * eagerly, records the whole sequence into a CUDA graph and replays it; later calls replay only.
+ * Families sharing a launch must admit one bitset filter count (every family's first four
+ * filters fit bitset rows).  Results are bit-identical to one pc_run_lease per window.
+ */
+int pc_multi_create(pc_ctx *ctx, const pc_focus *const *foci, uint32_t nfoci, const pc_filters *const *families,
+                    uint32_t nfam, const pc_window *windows, uint32_t nwin, const pc_tuning *tuning,
+                    uint64_t out_cap, pc_multi **out);
+int pc_multi_run(pc_ctx *ctx, pc_multi *m, uint32_t flags, pc_stats *stats);
+/* tile_base [nwin+1]: first subtile of each window; sizes [nwin x 2]: u and v list lengths;
+ * info[0..7]: subtiles, counters per subtile (stride), padded u entries, v entries, deep slice
+ * capacity, bitset filters, block words, threads. */
+int pc_multi_layout(const pc_multi *m, uint32_t *tile_base, uint64_t *sizes, uint64_t *info);
+/* Results of the last run: counts [subtiles x stride] (focused positions, the ng group survivors
+ * of the window's family, outputs, underflows), geometry [subtiles x 2], out [min(n_out, out_cap)
+ * x 2] with the global subtile in the high half of limb 1, as pc_run_batch. */
+int pc_multi_results(pc_ctx *ctx, const pc_multi *m, uint64_t *counts, uint64_t *geometry, uint64_t *out,
+                     uint64_t out_cap, uint64_t *n_out);
+int pc_multi_free(pc_ctx *ctx, pc_multi *m);
 
 /*
  * Plain per-position matcher over one tile: replaces Matcher.arrays' kernel (pseudocube/gpu.py:

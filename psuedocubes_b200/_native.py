@@ -24,14 +24,17 @@ PC_OK, PC_OVERFLOW, PC_INVALID, PC_ARITHMETIC, PC_TIMEOUT, PC_NOMEM, PC_CUDA = r
 SYMBOLS = ('pc_version', 'pc_device_count', 'pc_last_error', 'pc_init', 'pc_free', 'pc_mem_info',
            'pc_device_info', 'pc_sync', 'pc_mark', 'pc_elapsed', 'pc_buf_upload', 'pc_buf_download', 'pc_buf_size', 'pc_buf_free',
            'pc_buf_searchsorted', 'pc_focus_create', 'pc_focus_free', 'pc_focus_info', 'pc_focus_window',
-           'pc_filters_create', 'pc_filters_free', 'pc_run_batch', 'pc_run_lease', 'pc_run_plain',
+           'pc_filters_create', 'pc_filters_free', 'pc_run_batch', 'pc_run_lease', 'pc_multi_create',
+           'pc_multi_run', 'pc_multi_layout', 'pc_multi_results', 'pc_multi_free', 'pc_run_plain',
            'pc_run_plain_static', 'pc_selftest_wide')
+
+PC_RUN_GRAPH = 1
 
 
 class Tuning(ctypes.Structure):
     _fields_ = [('bitset_filters', ctypes.c_uint32), ('block_words', ctypes.c_uint32),
                 ('words_per_thread', ctypes.c_uint32), ('v_chunk', ctypes.c_uint32),
-                ('threads', ctypes.c_uint32), ('reserved', ctypes.c_uint32 * 3)]
+                ('threads', ctypes.c_uint32), ('deep_records', ctypes.c_uint32), ('reserved', ctypes.c_uint32 * 2)]
 
 
 class Stats(ctypes.Structure):
@@ -42,8 +45,17 @@ class Stats(ctypes.Structure):
     def as_dict(self) -> dict[str, Any]:
         return dict(kernel_ms=self.kernel_ms, bounds_ms=self.bounds_ms, window_ms=self.window_ms,
                     total_ms=self.total_ms, outputs=int(self.outputs), launches=int(self.launches),
-                    bitset_filters=int(self.reserved[0]), block_words=int(self.reserved[1]),
-                    threads=int(self.reserved[2]))
+                    deep_survivors=int(self.work_items), bitset_filters=int(self.reserved[0]),
+                    block_words=int(self.reserved[1]), threads=int(self.reserved[2]),
+                    cheap_filters=int(self.reserved[3]), graph=bool(self.reserved[4]))
+
+
+class Window(ctypes.Structure):
+    """One window of a multi-window launch (pc_window)."""
+    _fields_ = [('first', ctypes.c_uint64), ('end', ctypes.c_uint64), ('width', ctypes.c_uint64),
+                ('lo0', ctypes.c_uint64), ('lo1', ctypes.c_uint64), ('hi0', ctypes.c_uint64), ('hi1', ctypes.c_uint64),
+                ('focus_a', ctypes.c_uint32), ('focus_b', ctypes.c_uint32), ('family', ctypes.c_uint32),
+                ('reserved', ctypes.c_uint32)]
 
 
 _P = ctypes.c_void_p
@@ -90,6 +102,12 @@ def lib() -> ctypes.CDLL:
     so.pc_run_lease.argtypes = [_P, _P, _P, _P, ctypes.POINTER(Tuning), _U64, _U64, _U64,
                                 _U64, _U64, _U64, _U64, _U64P, _U64P, _U64P, _U64, ctypes.POINTER(_U64),
                                 ctypes.POINTER(Stats)]
+    so.pc_multi_create.argtypes = [_P, ctypes.POINTER(_P), _U32, ctypes.POINTER(_P), _U32, ctypes.POINTER(Window), _U32,
+                                   ctypes.POINTER(Tuning), _U64, pp]
+    so.pc_multi_run.argtypes = [_P, _P, _U32, ctypes.POINTER(Stats)]
+    so.pc_multi_layout.argtypes = [_P, _U32P, _U64P, _U64P]
+    so.pc_multi_results.argtypes = [_P, _P, _U64P, _U64P, _U64P, _U64, ctypes.POINTER(_U64)]
+    so.pc_multi_free.argtypes = [_P, _P]
     so.pc_run_plain.argtypes = [_P, _P, _P, _U64, _U64, _P, _U64, _U64, _U64, _U64, _U64, _U64,
                                 _U64P, _U64P, _U64, ctypes.POINTER(Stats)]
     so.pc_run_plain_static.argtypes = [ctypes.c_int, _U64P, _U64, _U64P, _U64, _U64, _U64, _U64, _U64, _U64, _U64,

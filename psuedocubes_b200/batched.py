@@ -1,0 +1,337 @@
+"""Batched uneven windows: many focus windows with different prime bounds in one launch sequence.
+
+The reference runs one tile (``Matcher.tile``, pseudocube/gpu.py:212-234) or one batch
+(``MaskedMatcher.run``, pseudocube/batch_experiment.py:239-248) per call.  Here a whole set of
+windows, each ``Window(p, first, end)`` with its own canonical v range and prime bound, is planned
+once (``WindowBatch``) and executed by one sequence of launches over the device-resident wheel
+tables: the u and v windows of every window are generated together, and stages 2 and 3 treat each
+window as a segment with its own interval, subtile width and residual filter family.  The
+sequence can be recorded into a CUDA graph and replayed (``run(graph=True)``).
+
+Per window, results carry the keys of the reference's plain tile path (``valid_focused_candidates``,
+``group_survivors``, ``all_values``, ``genuine_cubes``, ``cpu_confirmed_hits``, ``subtile_scopes``)
+and are identical to the plain per-tile loop over the same v range (``run_production.
+compute_batch``), whatever the subtile width: populations are sums over subtiles and outputs are
+the complete survivor set.
+
+``Autotuner`` picks the subtile width, the bitset tier (filters and block words), the threads per
+CTA and the survivor-buffer size for a workload by timing graph replays, and persists its choice
+per device and workload signature.
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import json
+import os
+import random
+import time
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Any, Iterable
+
+import numpy as np
+
+from . import _native as N
+from .batch_experiment import batch_result
+from .focus import A619, B619, Config
+from .gpu import MASK, Filters, GPUFocus, Runtime
+
+#: Prime bounds of the batched workload: the primes in [499, 619] that the reference accepts
+#: (``validate_p`` requires p = 1 mod 3).
+WORKLOAD_PRIMES = (499, 523, 541, 547, 571, 577, 601, 607, 613, 619)
+PRODUCTION_LO, PRODUCTION_HI = 10**27, 3 * 10**27
+
+
+@dataclass(frozen=True)
+class Window:
+    """One window: canonical v range [first, end) at prime bound p over (lo, hi], focus (A, B)."""
+    p: int
+    first: int
+    end: int
+    lo: int = PRODUCTION_LO
+    hi: int = PRODUCTION_HI
+    A: int = A619
+    B: int = B619
+
+    def config(self) -> Config:
+        return Config(self.p, self.lo, self.hi, self.A, self.B)
+
+
+def seeded_windows(count: int = 512, seed: int = 619003, span_exp: tuple[float, float] = (6.0, 10.0),
+                   primes: Iterable[int] = WORKLOAD_PRIMES) -> list[Window]:
+    """The batched workload: spans floor(10^U(lo, hi)) v, first uniform in [0, B - span), p uniform
+    over ``primes``, production interval and focus."""
+    rng = random.Random(seed)
+    choices = list(primes)
+    out = []
+    for _ in range(count):
+        span = int(10 ** rng.uniform(*span_exp))
+        first = rng.randrange(0, B619 - span)
+        out.append(Window(rng.choice(choices), first, first + span))
+    return out
+
+
+class BatchedEngine:
+    """Device-resident focus tables and filter families shared by every window batch of a runtime."""
+
+    def __init__(self, runtime: Runtime) -> None:
+        self.runtime = runtime
+        self._foci: dict[Any, GPUFocus] = {}
+        self._families: dict[tuple[int, int, int], Filters] = {}
+
+    def focus(self, focus: Any) -> GPUFocus:
+        key = (focus.modulus, focus.rings)
+        if key not in self._foci:
+            self._foci[key] = GPUFocus(self.runtime, focus)
+        return self._foci[key]
+
+    def family(self, config: Config) -> Filters:
+        key = (config.p, config.A, config.B)
+        if key not in self._families:
+            self._families[key] = Filters(self.runtime, config)
+        return self._families[key]
+
+    def plan(self, windows: list[Window], width: int = 100_000_000, tuning: dict[str, int] | None = None,
+             output_cap: int = 1 << 16) -> 'WindowBatch':
+        return WindowBatch(self, windows, width, tuning, output_cap)
+
+
+def _tuning(settings: dict[str, int] | None) -> N.Tuning:
+    t = N.Tuning()
+    for key, value in (settings or {}).items():
+        if key in ('bitset_filters', 'block_words', 'v_chunk', 'threads', 'deep_records'):
+            setattr(t, key, int(value))
+    return t
+
+
+class WindowBatch:
+    """A planned multi-window launch (pc_multi) with its device buffers."""
+
+    def __init__(self, engine: BatchedEngine, windows: list[Window], width: int,
+                 tuning: dict[str, int] | None, output_cap: int) -> None:
+        if not windows:
+            raise ValueError('empty window batch')
+        if width <= 0:
+            raise ValueError('subtile width must be positive')
+        rt = engine.runtime
+        self.runtime, self.engine, self.windows, self.width = rt, engine, list(windows), int(width)
+        self.output_cap = int(output_cap)
+        self.configs = [w.config() for w in self.windows]
+        foci: list[GPUFocus] = []
+        families: list[Filters] = []
+        index_f: dict[int, int] = {}
+        index_m: dict[int, int] = {}
+        spec = (N.Window * len(self.windows))()
+        for i, (w, c) in enumerate(zip(self.windows, self.configs)):
+            if not 0 <= w.first < w.end <= c.B:
+                raise ValueError('window outside the canonical domain')
+            af, bf = c.focuses()
+            ids = []
+            for focus in (af, bf):
+                g = engine.focus(focus)
+                if id(g) not in index_f:
+                    index_f[id(g)] = len(foci)
+                    foci.append(g)
+                ids.append(index_f[id(g)])
+            fam = engine.family(c)
+            if id(fam) not in index_m:
+                index_m[id(fam)] = len(families)
+                families.append(fam)
+            s = spec[i]
+            s.first, s.end, s.width = w.first, w.end, self.width
+            s.lo0, s.lo1, s.hi0, s.hi1 = c.lo & MASK, c.lo >> 64, c.hi & MASK, c.hi >> 64
+            s.focus_a, s.focus_b, s.family = ids[0], ids[1], index_m[id(fam)]
+        self.foci, self.families = foci, families
+        self._family_of = [index_m[id(engine.family(c))] for c in self.configs]
+        focus_ptrs = (ctypes.c_void_p * len(foci))(*[g.handle.value for g in foci])
+        family_ptrs = (ctypes.c_void_p * len(families))(*[f.handle.value for f in families])
+        self.tuning = _tuning(tuning)
+        handle = ctypes.c_void_p()
+        rt.check()
+        rt.call(rt.lib.pc_multi_create(rt.ctx, focus_ptrs, len(foci), family_ptrs, len(families), spec,
+                                       len(self.windows), ctypes.byref(self.tuning), self.output_cap,
+                                       ctypes.byref(handle)))
+        self.handle = handle
+        n = len(self.windows)
+        self.tile_base = np.zeros(n + 1, dtype=np.uint32)
+        self.sizes = np.zeros(2 * n, dtype=np.uint64)
+        info = np.zeros(8, dtype=np.uint64)
+        rt.lib.pc_multi_layout(handle, self.tile_base, self.sizes, info)
+        self.ntiles, self.stride = int(info[0]), int(info[1])
+        self.layout = dict(subtiles=self.ntiles, stride=self.stride, u_entries=int(info[2]), v_entries=int(info[3]),
+                           deep_records=int(info[4]), bitset_filters=int(info[5]), block_words=int(info[6]),
+                           threads=int(info[7]))
+        self.last_stats: dict[str, Any] = {}
+
+    def run(self, graph: bool = False) -> dict[str, Any]:
+        """Execute every window on the device (eager, or replay of the recorded graph) and return the
+        raw counters; ``results()`` turns them into per-window result dicts."""
+        rt = self.runtime
+        stats = N.Stats()
+        rt.check()
+        rt.call(rt.lib.pc_multi_run(rt.ctx, self.handle, N.PC_RUN_GRAPH if graph else 0, ctypes.byref(stats)))
+        self.last_stats = stats.as_dict()
+        return self.last_stats
+
+    def raw(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        rt = self.runtime
+        counts = np.zeros(max(1, self.ntiles * self.stride), dtype=np.uint64)
+        geometry = np.zeros(max(2, 2 * self.ntiles), dtype=np.uint64)
+        records = np.zeros(2 * max(1, self.output_cap), dtype=np.uint64)
+        n_out = ctypes.c_uint64()
+        rt.call(rt.lib.pc_multi_results(rt.ctx, self.handle, counts, geometry, records, self.output_cap,
+                                        ctypes.byref(n_out)))
+        return (counts[:self.ntiles * self.stride].reshape(self.ntiles, self.stride),
+                geometry[:2 * self.ntiles].reshape(self.ntiles, 2), records[:2 * n_out.value].reshape(-1, 2))
+
+    def positions(self) -> int:
+        """Focused candidate positions of the last run (all windows)."""
+        counts, _, _ = self.raw()
+        return int(counts[:, 0].sum())
+
+    def results(self) -> list[dict[str, Any]]:
+        """Per-window results of the last run, host-verified like the reference's tile results."""
+        counts, geometry, records = self.raw()
+        tile = (records[:, 1] >> np.uint64(32)).astype(np.int64) if len(records) else np.zeros(0, dtype=np.int64)
+        lo = records[:, 0] if len(records) else np.zeros(0, dtype=np.uint64)
+        hi = records[:, 1] & np.uint64(0xFFFFFFFF) if len(records) else np.zeros(0, dtype=np.uint64)
+        out = []
+        for i, (w, c) in enumerate(zip(self.windows, self.configs)):
+            t0, t1 = int(self.tile_base[i]), int(self.tile_base[i + 1])
+            fam = self.families[self._family_of[i]]
+            ng = fam.ng
+            pops = counts[t0:t1, :ng + 3]
+            per_tile: list[list[int]] = [[] for _ in range(t1 - t0)]
+            for k in np.nonzero((tile >= t0) & (tile < t1))[0].tolist():
+                per_tile[int(tile[k]) - t0].append(int(lo[k]) | (int(hi[k]) << 64))
+            for values in per_tile:
+                values.sort()
+            ranges = []
+            for v in range(w.first, w.end, self.width):
+                stop = min(v + self.width, w.end)
+                ranges.append((v, stop, c.u_interval(v)[0], c.u_interval(stop - 1)[1]))
+            geo = [(int(a), int(b)) for a, b in geometry[t0:t1]]
+            row = batch_result(c, ranges, pops, per_tile, geo, fam.filter_groups, 1 << 62)
+            row.update(p=w.p, first=str(w.first), end=str(w.end), focus_u=int(self.sizes[2 * i]),
+                       focus_v=int(self.sizes[2 * i + 1]))
+            out.append(row)
+        return out
+
+    def close(self) -> None:
+        if getattr(self, 'handle', None) and self.runtime.ctx:
+            self.runtime.lib.pc_multi_free(self.runtime.ctx, self.handle)
+            self.handle = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------------------------------
+# autotuner
+
+DEFAULT_SETTINGS: dict[str, int] = dict(width=1 << 26, bitset_filters=7, block_words=32, threads=768, deep_records=0)
+SEARCH_SPACE: dict[str, tuple[int, ...]] = dict(
+    width=(1 << 20, 1 << 22, 1 << 24, 1 << 26, 1 << 27),
+    bitset_filters=(5, 6, 7, 8),
+    block_words=(16, 32, 64),
+    threads=(512, 768, 1024),
+)
+
+
+def workload_signature(windows: list[Window]) -> str:
+    """Coarse description of a workload, stable across seeds of the same distribution."""
+    spans = sorted(w.end - w.first for w in windows)
+    total = sum(spans)
+    ps = sorted({w.p for w in windows})
+    return f'n{len(windows)}-span{len(str(total))}-median{len(str(spans[len(spans) // 2]))}-p{ps[0]}-{ps[-1]}'
+
+
+def tuning_path() -> Path:
+    env = os.environ.get('PSUEDOCUBES_TUNING')
+    if env:
+        return Path(env)
+    return Path.home() / '.cache' / 'psuedocubes_b200' / 'tuning.json'
+
+
+@dataclass
+class TuneResult:
+    settings: dict[str, int]
+    ms: float
+    trials: list[dict[str, Any]] = field(default_factory=list)
+
+
+class Autotuner:
+    """Coordinate search over subtile width, bitset filters, block words and threads, timed by
+    graph replays; the survivor buffer is then sized from the measured deep-survivor peak."""
+
+    def __init__(self, engine: BatchedEngine, path: Path | None = None, replays: int = 3) -> None:
+        self.engine, self.path, self.replays = engine, path or tuning_path(), replays
+
+    def key(self, windows: list[Window]) -> str:
+        return f'{self.engine.runtime.device_name}|{workload_signature(windows)}'
+
+    def load(self, windows: list[Window]) -> dict[str, int] | None:
+        try:
+            return json.loads(self.path.read_text()).get(self.key(windows))
+        except (OSError, ValueError):
+            return None
+
+    def save(self, windows: list[Window], settings: dict[str, int]) -> None:
+        try:
+            table = json.loads(self.path.read_text())
+        except (OSError, ValueError):
+            table = {}
+        table[self.key(windows)] = settings
+        self.path.parent.mkdir(parents=True, exist_ok=True)
+        self.path.write_text(json.dumps(table, indent=1, sort_keys=True))
+
+    def measure(self, windows: list[Window], settings: dict[str, int], output_cap: int) -> tuple[float, int]:
+        tuning = {k: v for k, v in settings.items() if k != 'width'}
+        batch = self.engine.plan(windows, settings['width'], tuning, output_cap)
+        try:
+            batch.run(graph=True)                         # eager run, capture, first replay
+            best = min(batch.run(graph=True)['kernel_ms'] for _ in range(self.replays))
+            return best, int(batch.last_stats.get('deep_survivors', 0))
+        finally:
+            batch.close()
+
+    def tune(self, windows: list[Window], output_cap: int = 1 << 16, reuse: bool = True) -> TuneResult:
+        if reuse:
+            known = self.load(windows)
+            if known:
+                return TuneResult(dict(known), float('nan'))
+        best = dict(DEFAULT_SETTINGS)
+        best_ms, deep = self.measure(windows, best, output_cap)
+        trials = [dict(best, ms=best_ms)]
+        for knob, values in SEARCH_SPACE.items():
+            for value in values:
+                if value == best[knob]:
+                    continue
+                trial = dict(best, **{knob: value})
+                try:
+                    ms, d = self.measure(windows, trial, output_cap)
+                except (ValueError, MemoryError) as exc:
+                    trials.append(dict(trial, error=str(exc)))
+                    continue
+                trials.append(dict(trial, ms=ms))
+                if ms < best_ms:
+                    best, best_ms, deep = trial, ms, d
+        # survivor buffer: the measured per-CTA peak with headroom, as a power of two
+        best['deep_records'] = max(1024, 1 << int(max(deep, 1) * 2 - 1).bit_length())
+        self.save(windows, best)
+        return TuneResult(best, best_ms, trials)
+
+
+def workload_digest(windows: list[Window]) -> str:
+    h = hashlib.sha256()
+    for w in windows:
+        h.update(f'{w.p},{w.first},{w.end},{w.lo},{w.hi},{w.A},{w.B};'.encode())
+    return h.hexdigest()
+
+
+__all__ = ['Window', 'WORKLOAD_PRIMES', 'seeded_windows', 'BatchedEngine', 'WindowBatch', 'Autotuner',
+           'DEFAULT_SETTINGS', 'SEARCH_SPACE', 'workload_signature', 'workload_digest', 'tuning_path']

@@ -42,6 +42,10 @@ void pc_release(pc_ctx *ctx, void *ptr, uint64_t bytes);
         if (e_ != cudaSuccess) return pc_cuda_fail((ctx), e_, #call);         \
     } while (0)
 
+inline int pc_cuda_status(pc_ctx *ctx, cudaError_t e, const char *what) {
+    return e == cudaSuccess ? PC_OK : pc_cuda_fail(ctx, e, what);
+}
+
 #define PC_LAUNCHED(ctx, what)                                                \
     do {                                                                      \
         cudaError_t e_ = cudaGetLastError();                                  \
@@ -188,3 +192,26 @@ __device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane) {
 // internal host helpers shared across translation units
 
 int pc_exclusive_scan_u64(pc_ctx *ctx, const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total_dev);
+uint64_t pc_scan_workspace(uint64_t n);
+int pc_exclusive_scan_ws(pc_ctx *ctx, const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total_dev,
+                         uint64_t *ws);
+
+// Many sorted focus windows generated together: one count launch, one scan and one emit launch.
+// Window i is written at base[i] of the shared output; each base is rounded up to a multiple of
+// the window's padding (so a u list can start on a block boundary of the matcher).
+struct WinBatch {
+    uint32_t n = 0;
+    uint64_t units = 0;
+    void *d_desc = nullptr, *d_foci = nullptr;
+    uint64_t *d_cnt = nullptr, *d_off = nullptr, *d_ws = nullptr, *d_tot = nullptr, *d_base = nullptr;
+    std::vector<uint64_t> total, base;
+    uint64_t out_len = 0;
+};
+struct pc_focus;
+uint64_t pc_focus_modulus(const pc_focus *f);
+int winbatch_plan(pc_ctx *ctx, Scratch &hold, const pc_focus *const *focus, const uint64_t *low, const uint64_t *high,
+                  const uint64_t *pad, uint32_t n, uint64_t cap, WinBatch &wb, int *launches);
+int winbatch_count(pc_ctx *ctx, const WinBatch &wb);
+int winbatch_emit(pc_ctx *ctx, const WinBatch &wb, uint64_t *out);
+int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, uint64_t cap, uint64_t **out,
+                   uint64_t *out_bytes, uint64_t *total_host, int *launches);

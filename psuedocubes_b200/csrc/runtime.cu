@@ -271,22 +271,32 @@ __global__ void k_scan_add(uint64_t *__restrict__ out, uint64_t n, const uint64_
         if (i < n) out[i] += add;
 }
 
+// Words of scratch the scan of n values needs (two arrays of tile sums per level).
+uint64_t pc_scan_workspace(uint64_t n) {
+    uint64_t words = 0;
+    for (;;) {
+        const uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+        words += 2 * (tiles + 1);
+        if (tiles <= 1) return words;
+        n = tiles;
+    }
+}
+
 // out[i] = sum in[0..i); *total_dev = sum of all (device pointer, may be null).  in may alias out.
-int pc_exclusive_scan_u64(pc_ctx *ctx, const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total_dev) {
+// ws holds pc_scan_workspace(n) words; nothing is allocated and nothing waits for the device, so
+// the scan can be recorded into a CUDA graph.
+int pc_exclusive_scan_ws(pc_ctx *ctx, const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total_dev,
+                         uint64_t *ws) {
     if (n == 0) {
         if (total_dev) PC_CHECK(ctx, cudaMemsetAsync(total_dev, 0, 8, ctx->stream));
         return PC_OK;
     }
-    uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
-    Scratch s(ctx);
-    uint64_t *sums, *sums_scan;
-    int rc = s.get(&sums, tiles + 1);
-    if (!rc) rc = s.get(&sums_scan, tiles + 1);
-    if (rc) return rc;
+    const uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    uint64_t *sums = ws, *sums_scan = ws + tiles + 1;
     k_scan_tiles<<<(unsigned)tiles, SCAN_T, 0, ctx->stream>>>(in, out, n, sums);
     PC_LAUNCHED(ctx, "scan tiles");
     if (tiles > 1) {
-        rc = pc_exclusive_scan_u64(ctx, sums, sums_scan, tiles, total_dev);
+        int rc = pc_exclusive_scan_ws(ctx, sums, sums_scan, tiles, total_dev, ws + 2 * (tiles + 1));
         if (rc) return rc;
         k_scan_add<<<(unsigned)tiles, SCAN_T, 0, ctx->stream>>>(out, n, sums_scan);
         PC_LAUNCHED(ctx, "scan add");
@@ -294,6 +304,14 @@ int pc_exclusive_scan_u64(pc_ctx *ctx, const uint64_t *in, uint64_t *out, uint64
         PC_CHECK(ctx, cudaMemcpyAsync(total_dev, sums, 8, cudaMemcpyDeviceToDevice, ctx->stream));
     }
     return PC_OK;
+}
+
+int pc_exclusive_scan_u64(pc_ctx *ctx, const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *total_dev) {
+    Scratch s(ctx);
+    uint64_t *ws;
+    int rc = s.get(&ws, pc_scan_workspace(n));
+    if (rc) return rc;
+    return pc_exclusive_scan_ws(ctx, in, out, n, total_dev, ws);
 }
 
 // ------------------------------------------------------------------------------------------

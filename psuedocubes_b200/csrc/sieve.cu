@@ -1,17 +1,20 @@
-// Stages 2 and 3: residue-bitset intersection and exact 128-bit later filters.
+// Stages 2 and 3: residue-bitset intersection and exact 128-bit later filters, over one or many
+// windows ("segments") in one launch sequence.
 //
-// Layout.  The sorted u list is cut into blocks of K words (32 u per word).  A work item is one
-// u block and a run of consecutive v rows whose exact u interval meets the block.  The CTA that
-// owns an item builds, in shared memory, the residue rows of the first NB residual filters for
-// its block (row r of filter q, bit i <=> allowed_q[(u_i B - r A) mod q]) and then streams its v
-// rows: each v reads the K-word rows selected by v mod q with 128-bit loads, ANDs them, counts
-// the group survivors by popcount, and constructs x = uB - vA only for the bits that survive
-// every bitset filter.  Those are tested exactly against the remaining filters in 128-bit
-// arithmetic.
+// Layout.  The sorted u lists of all segments are concatenated, each starting on a 2048-entry
+// boundary, and cut into blocks of K words (32 u per word); a block therefore belongs to exactly
+// one segment.  The v lists are concatenated unpadded.  A work item is one u block and a run of
+// consecutive v rows (of the block's segment) whose exact u interval meets the block.  The CTA
+// that owns an item builds, in shared memory, the residue rows of the first NB residual filters
+// of the segment's filter family for its block (row r of filter q, bit i <=> allowed_q[(u_i B -
+// r A) mod q]) and then streams its v rows: one lane per (v row, block) piece reads the K-word
+// rows selected by v mod q with 128-bit loads, ANDs them, counts the group survivors by
+// popcount, and queues the bits that survive every bitset filter.  Queued survivors are tested
+// by a warp against the next few filters from residues of u and v (the cheap tier); the rest go
+// to a per-CTA slice that k_deep finishes in exact 128-bit arithmetic.
 //
-// Rows are stored as 16-byte units with the unit index XOR-swizzled by the row index, so the
-// transposing writer (32 rows, one unit each) and the readers (one row, consecutive units) both
-// touch all banks once per wavefront.
+// Rows are stored unswizzled, K/4 16-byte units per row; lane l reads unit (l + p) mod (K/4) at
+// step p, so the 32 lanes of a warp spread evenly over the bank groups whatever rows they read.
 #include "common.cuh"
 #include <algorithm>
 #include <chrono>
@@ -24,24 +27,24 @@ struct FiltConst {
     uint32_t pad;
 };
 
-// Compact filter constants passed inside the kernel parameters (constant bank): fast remainder
-// constant, modulus, bitmap offset and 2^(16k) mod q for k = 1..5 (x < 2^96).
+// Compact filter constants: fast remainder constant, modulus, bitmap offset and 2^(16k) mod q for
+// k = 1..5 (x < 2^96).
 struct FiltC {
     uint64_t c;
     uint32_t q, tab_off;
     uint16_t r16[5];
     uint16_t pad[3];
 };
-constexpr int FC_INLINE = 128;
 
 struct pc_filters {
     uint64_t A = 0, B = 0;
     uint32_t nres = 0, ng = 0;
     std::vector<uint32_t> primes;
     FiltConst *d_fc = nullptr;
+    FiltC *d_fcs = nullptr;
     uint32_t *d_bits = nullptr;
-    uint32_t *d_pat = nullptr;       // swizzle-free RR patterns of the first filters (PATW words each)
-    uint64_t fc_bytes = 0, bits_bytes = 0, pat_bytes = 0;
+    uint32_t *d_pat = nullptr;       // rotation patterns of the first filters (PATW words each)
+    uint64_t fc_bytes = 0, fcs_bytes = 0, bits_bytes = 0, pat_bytes = 0;
     uint32_t nbmax = 0;              // filters usable as bitset rows
     uint32_t ainvb[PC_MAX_BITSET] = {};
     uint32_t rows_sum[PC_MAX_BITSET + 1] = {};   // prefix sums of q over the first filters
@@ -52,46 +55,50 @@ namespace {
 
 constexpr int PATW = 136;            // pattern words per bitset filter (q <= 2047)
 constexpr int TMAX_DEFAULT = 64;     // subtile counter slots per CTA
+constexpr uint64_t SEG_ALIGN = 2048; // u entries: every segment's u list starts on a block boundary
 
 struct __align__(16) VRec {
-    uint32_t left, right;            // exact u interval as indices into the sorted u list
+    uint32_t left, right;            // exact u interval as indices into the concatenated u list
     uint64_t v;
     uint16_t row[8];                 // row index (row0 + v mod q) of each bitset filter
 };
 
-struct MatchArgs {
-    const uint64_t *us;
-    const uint64_t *vs;
-    const VRec *rec;
-    uint64_t nu, nv;
+// One window: its focus moduli, interval, subtile geometry and slices of the concatenated lists.
+struct SegDev {
     uint64_t A, B;
     u128 lo, hi;
-    uint32_t nres, ng, nb;
-    uint32_t tmax;
-    const FiltConst *fc;
-    const uint32_t *bits;
-    const uint32_t *pat;
-    uint32_t q[PC_MAX_BITSET];
-    uint32_t row0[PC_MAX_BITSET];
-    uint32_t ainvb[PC_MAX_BITSET];
+    uint64_t v_first, width, v_end;
+    uint32_t u_off, nu, v_off, nv;
+    uint32_t tile_base, ntiles, fam, pad;
+};
+
+// One residual filter family (the filter list of one (p, A, B)) as the launch uses it: bitset
+// filters 0..NB-1, cheap-tier filters NB..NB+nch-1, the rest in k_deep.
+struct FamDev {
+    uint32_t nres, ng, total_rows, c2_live;   // c2_live: group 2 ends at the last bitset filter
+    uint32_t q[PC_MAX_BITSET], row0[PC_MAX_BITSET], ainvb[PC_MAX_BITSET];
     ModQ mq[PC_MAX_BITSET];
-    uint32_t total_rows;
-    uint64_t *counts;                // ntiles x (ng+3)
-    uint64_t *out;
-    uint64_t out_cap;
-    unsigned long long *n_out;
-    uint32_t ntiles;
+    uint32_t cq[PC_MAX_CHEAP], caq[PC_MAX_CHEAP], cbq[PC_MAX_CHEAP], cbits_off[PC_MAX_CHEAP];
+    ModQ cmq[PC_MAX_CHEAP];
+    uint8_t bgroup[16];              // group ended by filter idx (0 = none), idx < NB + nch
+    const uint32_t *pat;
+    const uint32_t *bits;
+    const FiltC *fcs;
+};
+
+struct MatchArgs {
+    const uint64_t *us;
+    const VRec *rec;
+    const SegDev *seg;
+    const FamDev *fam;
+    const uint32_t *blk_seg;         // per u block: its segment
+    uint32_t nch, tmax, stride;      // stride: counters per subtile (largest ng + 3)
+    uint32_t total_rows;             // largest over the families
+    uint64_t *counts;                // ntiles x stride
     const uint4 *bv;                 // per u block: v rows meeting it, v rows covering it
     const uint64_t *item_prefix;     // nblocks + 1
     uint64_t nblocks;
     const uint64_t *vchunk;          // device scalar
-    uint64_t v_first, width;         // subtile of v = (v - v_first) / width
-    // cheap tier: residual filters nb .. nb+nch-1 tested per survivor from residues of u and v
-    uint32_t nch;
-    uint32_t cq[PC_MAX_CHEAP], caq[PC_MAX_CHEAP], cbq[PC_MAX_CHEAP], cbits_off[PC_MAX_CHEAP];
-    ModQ cmq[PC_MAX_CHEAP];
-    uint8_t bgroup[16];              // group ended by filter idx (0 = none), idx < nb + nch
-    // deep tier: survivors of every cheap filter, appended to this CTA's slice
     uint4 *deep;                     // (v lo, v hi, u index, subtile) records
     uint32_t deep_cap;               // records per CTA slice
     uint32_t *deep_count;            // per CTA (may exceed deep_cap: the caller retries larger)
@@ -101,15 +108,15 @@ struct DeepArgs {
     const uint64_t *us;
     const uint4 *deep;
     const uint32_t *deep_count;
-    uint32_t deep_cap, slices;
-    uint64_t A, B;
-    uint32_t first, nres, ng, ntiles;          // filters first .. nres-1 remain
-    const uint32_t *bits;
+    uint32_t deep_cap, first, stride;        // filters first .. nres-1 remain
+    uint64_t ntiles;
+    const SegDev *seg;
+    const FamDev *fam;
+    const uint32_t *tile_seg;
     uint64_t *counts;
     uint64_t *out;
     uint64_t out_cap;
     unsigned long long *n_out;
-    FiltC fcs[FC_INLINE];
 };
 
 // first j with us[j] * B > key
@@ -133,24 +140,49 @@ __device__ __forceinline__ uint64_t lower_bound64(const uint64_t *__restrict__ a
     return lo;
 }
 
-__device__ __forceinline__ uint64_t tile_of(uint64_t v, uint64_t v_first, uint64_t width) {
-    uint64_t d = v - v_first;
+// Subtile of v inside a segment, floor((v - v_first) / width), or ntiles when v lies outside.
+// The double estimate is within one of the quotient (quotients are below 2^31), and the host
+// guarantees ntiles * width < 2^64.
+__device__ __forceinline__ uint64_t local_tile(uint64_t v, uint64_t v_first, uint64_t width, uint64_t ntiles) {
+    if (v < v_first) return ntiles;
+    const uint64_t d = v - v_first;
     uint64_t t = (uint64_t)((double)d / (double)width);
-    while (t * width > d) --t;
-    while ((t + 1) * width <= d) ++t;
+    if (t > ntiles) return ntiles;
+    if (t && t * width > d) --t;
+    if (t < ntiles && (t + 1) * width <= d) ++t;
     return t;
+}
+
+// Last segment whose list starts at or before index j (an empty segment shares its start with the
+// next one, so the search lands on the segment that holds j).
+__device__ __forceinline__ uint32_t seg_of_v(const SegDev *__restrict__ seg, uint32_t nseg, uint64_t j) {
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (seg[mid].v_off <= j) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t seg_of_u(const SegDev *__restrict__ seg, uint32_t nseg, uint64_t j) {
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (seg[mid].u_off <= j) lo = mid;
+        else hi = mid;
+    }
+    return lo;
 }
 
 struct PrepArgs {
     const uint64_t *us;
     const uint64_t *vs;
-    uint64_t nu, nv, A, B;
-    u128 lo, hi;
-    uint64_t v_first, width;
-    uint32_t ntiles, nb, ng;
-    uint32_t q[PC_MAX_BITSET];
-    uint32_t row0[PC_MAX_BITSET];
-    ModQ mq[PC_MAX_BITSET];
+    uint64_t nv;
+    const SegDev *seg;
+    uint32_t nseg;
+    const FamDev *fam;
+    uint32_t nb, stride;
     VRec *rec;
     uint64_t *counts;
     unsigned long long *bad;
@@ -158,8 +190,8 @@ struct PrepArgs {
 
 // Per v row: exact u interval as list indices (batch_experiment.py:209-215), bitset row
 // indices, and the focused-position count of its subtile.  A thread owns PREP_RUN consecutive v
-// rows: one binary search per bound for the first, then the monotone bounds advance linearly
-// (about N_u/N_v < 1 step per row).
+// rows: one binary search per bound for the first row of each segment, then the monotone bounds
+// advance linearly (about N_u/N_v < 1 step per row).
 constexpr int PREP_RUN = 16;
 
 __device__ __forceinline__ uint64_t advance_le(const uint64_t *__restrict__ us, uint64_t n, uint64_t B, u128 key,
@@ -176,33 +208,40 @@ __global__ void k_vprep(const PrepArgs a) {
     const uint64_t j0 = t * PREP_RUN;
     if (j0 >= a.nv) return;
     const uint64_t j1 = umin64(a.nv, j0 + PREP_RUN);
+    uint32_t s = seg_of_v(a.seg, a.nseg, j0);
     uint64_t left = 0, right = 0, tile = UINT64_MAX, t_lo = 1, t_hi = 0, pop = 0;
+    bool fresh = true;
     for (uint64_t j = j0; j < j1; ++j) {
+        while (s + 1 < a.nseg && j >= (uint64_t)a.seg[s].v_off + a.seg[s].nv) {
+            ++s;
+            fresh = true;
+        }
+        const SegDev &g = a.seg[s];
+        const FamDev &F = a.fam[g.fam];
+        const uint64_t u0 = g.u_off, u1 = u0 + g.nu;
         const uint64_t v = a.vs[j];
-        const u128 shift = mul_wide(v, a.A);
-        const u128 klo = add128(shift, a.lo), khi = add128(shift, a.hi);
-        if (j == j0) {
-            left = count_le(a.us, a.nu, a.B, klo);
-            right = umax64(left, count_le(a.us, a.nu, a.B, khi));
+        const u128 shift = mul_wide(v, g.A);
+        const u128 klo = add128(shift, g.lo), khi = add128(shift, g.hi);
+        if (fresh) {
+            left = u0 + count_le(a.us + u0, g.nu, g.B, klo);
+            right = umax64(left, u0 + count_le(a.us + u0, g.nu, g.B, khi));
+            t_lo = 1, t_hi = 0;                           // force a subtile lookup
+            fresh = false;
         } else {
-            left = advance_le(a.us, a.nu, a.B, klo, left);
-            right = advance_le(a.us, a.nu, a.B, khi, umax64(left, right));
+            left = advance_le(a.us, u1, g.B, klo, left);
+            right = advance_le(a.us, u1, g.B, khi, umax64(left, right));
         }
         if (v < t_lo || v >= t_hi) {
-            if (tile != UINT64_MAX && pop)
-                atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3)], (unsigned long long)pop);
+            if (tile != UINT64_MAX && pop) atomicAdd((unsigned long long *)&a.counts[tile * a.stride], (unsigned long long)pop);
             pop = 0;
-            if (v < a.v_first) {
+            const uint64_t lt = local_tile(v, g.v_first, g.width, g.ntiles);
+            if (lt >= g.ntiles) {
                 atomicAdd(a.bad, 1ull);
                 tile = UINT64_MAX, t_lo = 1, t_hi = 0;
             } else {
-                tile = tile_of(v, a.v_first, a.width);
-                t_lo = a.v_first + tile * a.width;
-                t_hi = t_lo + a.width;
-                if (tile >= a.ntiles) {
-                    atomicAdd(a.bad, 1ull);
-                    tile = UINT64_MAX, t_lo = 1, t_hi = 0;
-                }
+                tile = g.tile_base + lt;
+                t_lo = g.v_first + lt * g.width;
+                t_hi = t_lo + g.width;
             }
         }
         VRec r;
@@ -211,32 +250,33 @@ __global__ void k_vprep(const PrepArgs a) {
         r.v = v;
 #pragma unroll
         for (int f = 0; f < PC_MAX_BITSET; ++f)
-            r.row[f] = f < (int)a.nb ? (uint16_t)(a.row0[f] + mod64(v, a.mq[f])) : (uint16_t)0;
+            r.row[f] = f < (int)a.nb ? (uint16_t)(F.row0[f] + mod64(v, F.mq[f])) : (uint16_t)0;
         a.rec[j] = r;
         pop += right - left;
     }
-    if (tile != UINT64_MAX && pop) atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3)], (unsigned long long)pop);
+    if (tile != UINT64_MAX && pop) atomicAdd((unsigned long long *)&a.counts[tile * a.stride], (unsigned long long)pop);
 }
 
 // Per subtile: u count and v count of its envelope (searchsorted bounds of
 // batch_experiment.py:37-43, as list-independent differences).
-__global__ void k_geometry(const uint64_t *__restrict__ us, uint64_t nu, const uint64_t *__restrict__ vs, uint64_t nv,
-                           uint64_t A, uint64_t B, u128 lo, u128 hi, uint64_t v_first, uint64_t width,
-                           uint64_t v_end, uint32_t ntiles, uint64_t *__restrict__ geometry) {
-    uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (s >= ntiles) return;
-    uint64_t first = v_first + s * width;
-    uint64_t end = min(first + width, v_end);
-    uint64_t ua = count_le(us, nu, B, add128(mul_wide(first, A), lo));
-    uint64_t ub = count_le(us, nu, B, add128(mul_wide(end - 1, A), hi));
-    uint64_t va = lower_bound64(vs, nv, first), vb = lower_bound64(vs, nv, end);
-    geometry[2 * s] = ub > ua ? ub - ua : 0;
-    geometry[2 * s + 1] = vb - va;
+__global__ void k_geometry(const uint64_t *__restrict__ us, const uint64_t *__restrict__ vs, const SegDev *__restrict__ seg,
+                           const uint32_t *__restrict__ tile_seg, uint64_t ntiles, uint64_t *__restrict__ geometry) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    const SegDev &g = seg[tile_seg[t]];
+    const uint64_t first = g.v_first + (t - g.tile_base) * g.width;
+    const uint64_t end = umin64(first + g.width, g.v_end);
+    const uint64_t *su = us + g.u_off, *sv = vs + g.v_off;
+    const uint64_t ua = count_le(su, g.nu, g.B, add128(mul_wide(first, g.A), g.lo));
+    const uint64_t ub = count_le(su, g.nu, g.B, add128(mul_wide(end - 1, g.A), g.hi));
+    const uint64_t va = lower_bound64(sv, g.nv, first), vb = lower_bound64(sv, g.nv, end);
+    geometry[2 * t] = ub > ua ? ub - ua : 0;
+    geometry[2 * t + 1] = vb - va;
 }
 
 // Per u block of UB entries: [va, vb) of v rows whose [left, right) meets the block, and the
 // sub-range [f0, f1) of rows covering the whole block (left <= start and right >= stop); left and
-// right are monotone in the row index, so all four are binary searches.
+// right are monotone in the row index within a segment, so all four are binary searches.
 __device__ __forceinline__ uint64_t first_right_ge(const VRec *__restrict__ rec, uint64_t lo, uint64_t hi, uint64_t x) {
     while (lo < hi) {
         uint64_t mid = lo + (hi - lo) / 2;
@@ -255,13 +295,25 @@ __device__ __forceinline__ uint64_t first_left_ge(const VRec *__restrict__ rec, 
     return lo;
 }
 
-__global__ void k_blocks(const VRec *__restrict__ rec, uint64_t nv, uint64_t nu, uint32_t UB, uint64_t nblocks,
-                         uint4 *__restrict__ bv, uint64_t *__restrict__ pieces) {
-    uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+__global__ void k_blocks(const VRec *__restrict__ rec, const SegDev *__restrict__ seg, uint32_t nseg, uint32_t UB,
+                         uint64_t nblocks, uint4 *__restrict__ bv, uint32_t *__restrict__ blk_seg,
+                         uint64_t *__restrict__ pieces) {
+    const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (b >= nblocks) return;
-    const uint64_t start = b * UB, stop = umin64(nu, start + UB);
-    const uint64_t va = first_right_ge(rec, 0, nv, start + 1);
-    const uint64_t vb = first_left_ge(rec, va, nv, stop);
+    const uint64_t start = b * UB;
+    const uint32_t s = seg_of_u(seg, nseg, start);
+    const SegDev &g = seg[s];
+    const uint64_t u_end = (uint64_t)g.u_off + g.nu;
+    blk_seg[b] = s;
+    if (start >= u_end) {                                 // padding between segments
+        bv[b] = make_uint4(0, 0, 0, 0);
+        pieces[b] = 0;
+        return;
+    }
+    const uint64_t stop = umin64(u_end, start + UB);
+    const uint64_t r0 = g.v_off, r1 = r0 + g.nv;
+    const uint64_t va = first_right_ge(rec, r0, r1, start + 1);
+    const uint64_t vb = first_left_ge(rec, va, r1, stop);
     uint64_t f0 = umax64(va, first_right_ge(rec, va, vb, stop));
     uint64_t f1 = umin64(vb, first_left_ge(rec, va, vb, start + 1));
     if (f1 < f0) f1 = f0;
@@ -295,78 +347,82 @@ struct Geo {
     __device__ static __forceinline__ uint32_t unit(uint32_t row, uint32_t c) { return row * U + c; }
 };
 
+// Residue rows of the family's first NB filters for one block (entries >= n_valid are zero), and
+// the residues u*B mod q of its cheap-tier filters.
 template <int NB, int K>
-__device__ void build_rows(const MatchArgs &a, uint4 *__restrict__ rows, uint16_t *__restrict__ ures,
-                           const uint32_t *__restrict__ pat_s, uint32_t block_u0, uint32_t lane, uint32_t warp,
-                           uint32_t nwarps) {
+__device__ void build_rows(const uint64_t *__restrict__ us, const FamDev &F, uint32_t nch, uint4 *__restrict__ rows,
+                           uint16_t *__restrict__ ures, const uint32_t *__restrict__ pat_s, uint32_t block_u0,
+                           uint32_t n_valid, uint32_t lane, uint32_t warp, uint32_t nwarps) {
     using G = Geo<K>;
-    const uint64_t *ub = a.us + block_u0;
-    // residues u*B mod q of the cheap-tier filters, one per block entry
+    const uint64_t *ub = us + block_u0;
     for (uint32_t k = threadIdx.x; k < G::UB; k += blockDim.x) {
-        const bool valid = block_u0 + k < a.nu;
-        const uint64_t u = valid ? __ldg(ub + k) : 0;
-        for (uint32_t t = 0; t < a.nch; ++t)
-            ures[t * G::UB + k] = (uint16_t)fastmod32(mod64(u, a.cmq[t]) * a.cbq[t], a.cmq[t].c, a.cq[t]);
+        const uint64_t u = k < n_valid ? __ldg(ub + k) : 0;
+        for (uint32_t t = 0; t < nch; ++t)
+            ures[t * G::UB + k] = (uint16_t)fastmod32(mod64(u, F.cmq[t]) * F.cbq[t], F.cmq[t].c, F.cq[t]);
     }
     // a warp builds all q rows of one filter for one 16-byte unit (4 words = 128 u)
     for (uint32_t pair = warp; pair < NB * G::U; pair += nwarps) {
-        uint32_t f = pair / G::U, c = pair % G::U;
-        const uint32_t q = a.q[f];
+        const uint32_t f = pair / G::U, c = pair % G::U;
+        const uint32_t q = F.q[f];
         uint32_t t[4];
         bool valid[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            uint32_t local = (c * 4 + k) * 32 + lane;
-            valid[k] = block_u0 + local < a.nu;
-            uint32_t um = valid[k] ? mod64(__ldg(ub + local), a.mq[f]) : 0;
-            t[k] = fastmod32(um * a.ainvb[f], a.mq[f].c, q);
+            const uint32_t local = (c * 4 + k) * 32 + lane;
+            valid[k] = local < n_valid;
+            const uint32_t um = valid[k] ? mod64(__ldg(ub + local), F.mq[f]) : 0;
+            t[k] = fastmod32(um * F.ainvb[f], F.mq[f].c, q);
         }
         const uint32_t *p = pat_s + f * PATW;
+        const uint32_t row0 = F.row0[f];
         for (uint32_t g = 0; g * 32 < q; ++g) {
             uint32_t w[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                uint32_t st = 32 * g + q - t[k];
-                uint32_t col = __funnelshift_r(p[st >> 5], p[(st >> 5) + 1], st & 31);
+                const uint32_t st = 32 * g + q - t[k];
+                const uint32_t col = __funnelshift_r(p[st >> 5], p[(st >> 5) + 1], st & 31);
                 w[k] = transpose32(valid[k] ? col : 0u, lane);
             }
-            uint32_t r = 32 * g + lane;
-            if (r < q) {
-                uint32_t row = a.row0[f] + r;
-                rows[G::unit(row, c)] = make_uint4(w[0], w[1], w[2], w[3]);
-            }
+            const uint32_t r = 32 * g + lane;
+            if (r < q) rows[G::unit(row0 + r, c)] = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 }
 
-constexpr int CBW = 64;   // bitmap words per cheap-tier filter (q <= 2047)
-
-// Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.
-constexpr int QCAP = 64;              // survivor ring per warp (pending < 64 by construction)
+constexpr int CBW = 64;                 // bitmap words per cheap-tier filter (q <= 2047)
+constexpr int QCAP = 64;                // survivor ring per warp (pending < 64 by construction)
 constexpr uint32_t SLOT_FAR = 0xFFFFF;  // queued slot too large to encode: the drain recomputes it
+
+__host__ __device__ constexpr uint32_t round16(uint32_t x) { return (x + 15) & ~15u; }
 
 // Shared-memory layout of k_match (byte offsets); every region starts 16-byte aligned.  The
 // residue-row patterns are only read while rows are built, when every survivor ring is empty,
 // so they share the rings' space.
 struct MatchSmem {
-    uint32_t rows, ures, qv, qm, pat, cbits, cnt, misc, total;
+    uint32_t rows, ures, qv, qm, pat, cbits, cnt, fam, seg, misc, total;
     __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t nch, uint32_t tmax,
                                   uint32_t ng, uint32_t warps) {
         rows = 0;
         ures = rows + total_rows * (K / 4) * 16;
-        qv = ures + ((nch * K * 32 * 2 + 15) & ~15u);
+        qv = ures + round16(nch * K * 32 * 2);
         qm = qv + warps * QCAP * 8;
         pat = qv;
         const uint32_t ring_end = qm + warps * QCAP * 4, pat_end = pat + nb * PATW * 4;
-        cbits = ((ring_end > pat_end ? ring_end : pat_end) + 15) & ~15u;
+        cbits = round16(ring_end > pat_end ? ring_end : pat_end);
         cnt = cbits + nch * CBW * 4;
-        misc = cnt + ((tmax * (ng + 2) * 4 + 15) & ~15u);
+        fam = cnt + round16(tmax * (ng + 2) * 4);
+        seg = fam + round16(sizeof(FamDev));
+        misc = seg + round16(sizeof(SegDev));
         total = misc + 16;
     }
 };
 
 __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bits [lo, hi) of one 32-bit word
     return low_bits((uint32_t)min(max(hi, 0), 32)) & ~low_bits((uint32_t)min(max(lo, 0), 32));
+}
+
+__device__ __forceinline__ void copy_words(void *dst, const void *src, uint32_t bytes) {
+    for (uint32_t i = threadIdx.x; i < bytes / 4; i += blockDim.x) ((uint32_t *)dst)[i] = ((const uint32_t *)src)[i];
 }
 
 // One lane owns one (v row, u block) piece: it walks the block's K/4 16-byte units in the order
@@ -379,7 +435,8 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     constexpr uint32_t U = G::U;
     extern __shared__ uint4 smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const MatchSmem L(a.total_rows, K, NB, a.nch, a.tmax, a.ng, nwarps);
+    const uint32_t ngmax = a.stride - 3;
+    const MatchSmem L(a.total_rows, K, NB, a.nch, a.tmax, ngmax, nwarps);
     char *base = (char *)smem;
     const uint4 *rows = (const uint4 *)(base + L.rows);
     uint16_t *ures = (uint16_t *)(base + L.ures);
@@ -387,15 +444,13 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     uint32_t *qm = (uint32_t *)(base + L.qm) + warp * QCAP;
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
     uint32_t *cbits = (uint32_t *)(base + L.cbits);
-    uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ng+2): groups 1..ng, outputs
+    uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ngmax+2): groups 1..ng
+    FamDev &F = *(FamDev *)(base + L.fam);
+    SegDev &S = *(SegDev *)(base + L.seg);
     uint32_t *deep_ctr = (uint32_t *)(base + L.misc);
-    const uint32_t stride = a.ng + 2;
+    const uint32_t cstride = ngmax + 2;
 
     const uint32_t lanes_below = (1u << lane) - 1u;
-    for (uint32_t i = threadIdx.x; i < a.nch * CBW; i += blockDim.x) {
-        const uint32_t t = i / CBW, w = i % CBW;
-        cbits[i] = w * 32 < a.cq[t] ? a.bits[a.cbits_off[t] + w] : 0u;
-    }
     if (threadIdx.x == 0) *deep_ctr = 0;
     uint4 *deep_slice = a.deep + (size_t)blockIdx.x * a.deep_cap;
 
@@ -403,6 +458,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     const uint64_t vch = *a.vchunk;
     const uint64_t i0 = n_items * blockIdx.x / gridDim.x, i1 = n_items * (blockIdx.x + 1) / gridDim.x;
     uint64_t cur = UINT64_MAX, bsearch = 0;
+    uint32_t cur_seg = UINT32_MAX, cur_fam = UINT32_MAX;
     if (i0 < i1) {                                        // block of the first item: last b with prefix[b] <= i0
         uint64_t lo = 0, hi = a.nblocks;
         while (hi - lo > 1) {
@@ -412,7 +468,6 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         }
         bsearch = lo;
     }
-    const bool c2_live = NB == 8 || (NB > 4 && NB == (int)a.nres);
     const uint32_t nch = a.nch;
 
     for (uint64_t it = i0; it < i1; ++it) {
@@ -427,14 +482,34 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         const uint32_t block_u0 = (uint32_t)(b * G::UB);
         __syncthreads();                                  // previous item finished with shared memory
         if (b != cur) {
-            for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = a.pat[i];
+            const uint32_t sg = a.blk_seg[b];
+            if (sg != cur_seg) {
+                const uint32_t fm = a.seg[sg].fam;
+                copy_words(&S, a.seg + sg, sizeof(SegDev));
+                if (fm != cur_fam) copy_words(&F, a.fam + fm, sizeof(FamDev));
+                __syncthreads();
+                if (fm != cur_fam) {
+                    for (uint32_t i = threadIdx.x; i < nch * CBW; i += blockDim.x) {
+                        const uint32_t t = i / CBW, w = i % CBW;
+                        cbits[i] = w * 32 < F.cq[t] ? F.bits[F.cbits_off[t] + w] : 0u;
+                    }
+                }
+                cur_seg = sg;
+                cur_fam = fm;
+            }
+            for (uint32_t i = threadIdx.x; i < NB * PATW; i += blockDim.x) pat_s[i] = F.pat[i];
             __syncthreads();
-            build_rows<NB, K>(a, (uint4 *)rows, ures, pat_s, block_u0, lane, warp, nwarps);
+            const uint32_t u_end = S.u_off + S.nu;
+            const uint32_t n_valid = u_end > block_u0 ? min(u_end - block_u0, (uint32_t)G::UB) : 0u;
+            build_rows<NB, K>(a.us, F, nch, (uint4 *)rows, ures, pat_s, block_u0, n_valid, lane, warp, nwarps);
             cur = b;
         }
-        for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) cnt_s[k] = 0;
+        for (uint32_t k = threadIdx.x; k < a.tmax * cstride; k += blockDim.x) cnt_s[k] = 0;
         __syncthreads();
-        const uint64_t tile_base = tile_of(a.rec[va].v, a.v_first, a.width);
+        const uint64_t sv_first = S.v_first, swidth = S.width, stn = S.ntiles, stb = S.tile_base;
+        const uint64_t seg_tiles_end = stb + stn;
+        const bool c2_live = F.c2_live != 0;
+        const uint64_t tile_base = stb + local_tile(a.rec[va].v, sv_first, swidth, stn);
 
         uint32_t c[3] = {0, 0, 0};
         uint64_t ctile = UINT64_MAX, t_lo = 1, t_hi = 0;  // this lane's subtile and its v range
@@ -448,9 +523,9 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                 const uint32_t sum = __reduce_add_sync(same, c[g]);
                 if (key == ctile && lane == leader && sum) {
                     const uint64_t slot = ctile - tile_base;
-                    if (slot < a.tmax) atomicAdd(cnt_s + slot * stride + 1 + g, sum);
-                    else if (ctile < a.ntiles)
-                        atomicAdd((unsigned long long *)&a.counts[ctile * (a.ng + 3) + 1 + g], (unsigned long long)sum);
+                    if (slot < a.tmax) atomicAdd(cnt_s + slot * cstride + 1 + g, sum);
+                    else if (ctile < seg_tiles_end)
+                        atomicAdd((unsigned long long *)&a.counts[ctile * a.stride + 1 + g], (unsigned long long)sum);
                 }
                 c[g] = 0;
             }
@@ -473,17 +548,17 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             qhead += n;
             if (!mine) return;
             const uint32_t uidx = meta & 0xfff, slot = meta >> 12;
-            const uint64_t tile = slot == SLOT_FAR ? tile_of(v, a.v_first, a.width) : tile_base + slot;
+            const uint64_t tile = slot == SLOT_FAR ? stb + local_tile(v, sv_first, swidth, stn) : tile_base + slot;
+            if (tile >= seg_tiles_end) return;            // v outside the subtile geometry (reported by k_vprep)
             for (uint32_t t = 0; t < nch; ++t) {
-                const uint32_t vr = fastmod32(mod64(v, a.cmq[t]) * a.caq[t], a.cmq[t].c, a.cq[t]);
+                const uint32_t vr = fastmod32(mod64(v, F.cmq[t]) * F.caq[t], F.cmq[t].c, F.cq[t]);
                 int32_t m = (int32_t)ures[t * G::UB + uidx] - (int32_t)vr;
-                if (m < 0) m += (int32_t)a.cq[t];
+                if (m < 0) m += (int32_t)F.cq[t];
                 if (!((cbits[t * CBW + (m >> 5)] >> (m & 31)) & 1u)) return;
-                const uint32_t g = a.bgroup[NB + t];
+                const uint32_t g = F.bgroup[NB + t];
                 if (g) {
-                    if (slot < a.tmax) atomicAdd(cnt_s + slot * stride + g, 1u);
-                    else if (tile < a.ntiles)
-                        atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], 1ull);
+                    if (slot < a.tmax) atomicAdd(cnt_s + slot * cstride + g, 1u);
+                    else atomicAdd((unsigned long long *)&a.counts[tile * a.stride + g], 1ull);
                 }
             }
             const uint32_t at = atomicAdd(deep_ctr, 1u);
@@ -512,14 +587,15 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             if (__any_sync(0xffffffffu, moved)) {
                 flush();
                 if (moved) {
-                    ctile = tile_of(rec.v, a.v_first, a.width);
-                    t_lo = a.v_first + ctile * a.width;
-                    t_hi = t_lo + a.width;
+                    const uint64_t lt = local_tile(rec.v, sv_first, swidth, stn);
+                    ctile = lt < stn ? stb + lt : UINT64_MAX;
+                    t_lo = sv_first + lt * swidth;
+                    t_hi = lt < stn ? t_lo + swidth : t_lo;
                 }
             }
             uint32_t ro[NB];                              // unit offset of each filter's row
 #pragma unroll
-            for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)(active ? rec.row[f] : a.row0[f]) * U;
+            for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)(active ? rec.row[f] : 0) * U;
             const uint64_t slot64 = ctile - tile_base;
             const uint32_t meta_hi = (slot64 < SLOT_FAR ? (uint32_t)slot64 : SLOT_FAR) << 12;
 
@@ -577,13 +653,13 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         if (qtail != qhead) drain(qtail - qhead);
         flush();
         __syncthreads();
-        for (uint32_t k = threadIdx.x; k < a.tmax * stride; k += blockDim.x) {
-            uint32_t cv = cnt_s[k];
+        for (uint32_t k = threadIdx.x; k < a.tmax * cstride; k += blockDim.x) {
+            const uint32_t cv = cnt_s[k];
             if (cv) {
-                uint32_t slot = k / stride, g = k % stride;
-                uint64_t tile = tile_base + slot;
-                if (tile < a.ntiles)
-                    atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + g], (unsigned long long)cv);
+                const uint32_t slot = k / cstride, g = k % cstride;
+                const uint64_t tile = tile_base + slot;
+                if (tile < seg_tiles_end)
+                    atomicAdd((unsigned long long *)&a.counts[tile * a.stride + g], (unsigned long long)cv);
             }
         }
     }
@@ -599,8 +675,8 @@ __device__ __forceinline__ uint32_t mod_limbs(const uint32_t h[6], const FiltC &
 }
 
 // Exact later filters on every deep record: x = uB - vA in two 64-bit limbs, filters first..nres-1
-// with group counters, then the output record.  One record per thread; outputs are appended with
-// one atomic per warp.
+// of the record's family with group counters, then the output record.  One record per thread;
+// outputs are appended with one atomic per warp.
 __global__ void __launch_bounds__(256) k_deep(const DeepArgs a) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lanes_below = (1u << lane) - 1u;
@@ -609,33 +685,40 @@ __global__ void __launch_bounds__(256) k_deep(const DeepArgs a) {
     for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
         const uint32_t at = base + threadIdx.x;
         const uint64_t i = (uint64_t)slice * a.deep_cap + at;
-        const bool mine = at < count;
         bool pass = false;
         u128 x{0, 0};
         uint64_t tile = 0;
-        if (mine) {
+        uint32_t ng = 0;
+        if (at < count) {
             const uint4 r = a.deep[i];
             const uint64_t v = (uint64_t)r.y << 32 | r.x;
             tile = r.w;
-            const u128 pos = mul_wide(__ldg(a.us + r.z), a.B), shift = mul_wide(v, a.A);
-            if (tile >= a.ntiles) {
-            } else if (less128(pos, shift)) {
-                atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 2], 1ull);
-            } else {
-                x = sub128(pos, shift);
-                const uint32_t h[6] = {(uint32_t)x.lo & 0xffffu, (uint32_t)(x.lo >> 16) & 0xffffu,
-                                       (uint32_t)(x.lo >> 32) & 0xffffu, (uint32_t)(x.lo >> 48),
-                                       (uint32_t)x.hi & 0xffffu, (uint32_t)(x.hi >> 16) & 0xffffu};
-                pass = true;
-                for (uint32_t idx = a.first; idx < a.nres; ++idx) {
-                    const FiltC f = a.fcs[idx];
-                    const uint32_t m = mod_limbs(h, f);
-                    if (!((__ldg(a.bits + f.tab_off + (m >> 5)) >> (m & 31)) & 1u)) {
-                        pass = false;
-                        break;
+            if (tile < a.ntiles) {
+                const SegDev &g = a.seg[a.tile_seg[tile]];
+                const FamDev &F = a.fam[g.fam];
+                ng = F.ng;
+                const u128 pos = mul_wide(__ldg(a.us + r.z), g.B), shift = mul_wide(v, g.A);
+                if (less128(pos, shift)) {
+                    atomicAdd((unsigned long long *)&a.counts[tile * a.stride + ng + 2], 1ull);
+                } else {
+                    x = sub128(pos, shift);
+                    const uint32_t h[6] = {(uint32_t)x.lo & 0xffffu, (uint32_t)(x.lo >> 16) & 0xffffu,
+                                           (uint32_t)(x.lo >> 32) & 0xffffu, (uint32_t)(x.lo >> 48),
+                                           (uint32_t)x.hi & 0xffffu, (uint32_t)(x.hi >> 16) & 0xffffu};
+                    pass = true;
+                    const uint32_t nres = F.nres;
+                    const FiltC *fcs = F.fcs;
+                    const uint32_t *bits = F.bits;
+                    for (uint32_t idx = a.first; idx < nres; ++idx) {
+                        const FiltC f = fcs[idx];
+                        const uint32_t m = mod_limbs(h, f);
+                        if (!((__ldg(bits + f.tab_off + (m >> 5)) >> (m & 31)) & 1u)) {
+                            pass = false;
+                            break;
+                        }
+                        if ((idx & 3) == 3 || idx + 1 == nres)
+                            atomicAdd((unsigned long long *)&a.counts[tile * a.stride + idx / 4 + 1], 1ull);
                     }
-                    if ((idx & 3) == 3 || idx + 1 == a.nres)
-                        atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + idx / 4 + 1], 1ull);
                 }
             }
         }
@@ -648,8 +731,7 @@ __global__ void __launch_bounds__(256) k_deep(const DeepArgs a) {
             if (pass) {
                 const uint32_t same = __match_any_sync(won, tile);
                 if (lane == (uint32_t)(__ffs(same) - 1))
-                    atomicAdd((unsigned long long *)&a.counts[tile * (a.ng + 3) + a.ng + 1],
-                              (unsigned long long)__popc(same));
+                    atomicAdd((unsigned long long *)&a.counts[tile * a.stride + ng + 1], (unsigned long long)__popc(same));
                 const unsigned long long o = first + __popc(won & lanes_below);
                 if (o < a.out_cap) {
                     a.out[2 * o] = x.lo;
@@ -720,35 +802,38 @@ __global__ void __launch_bounds__(256) k_plain(const PlainArgs a) {
 }
 
 template <int NB, int K, int NT>
-int launch_match_t(pc_ctx *ctx, const MatchArgs &a, size_t smem, int grid) {
+int launch_match_t(pc_ctx *ctx, const MatchArgs &a, size_t smem, int grid, int mode) {
     auto kern = k_match<NB, K, NT>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return pc_cuda_fail(ctx, e, "match smem attribute");
+    if (mode != 1) {       // 0: attribute and launch, 1: launch only (inside a capture), 2: attribute only
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return pc_cuda_fail(ctx, e, "match smem attribute");
+        if (mode == 2) return PC_OK;
+    }
     kern<<<grid, NT, smem, ctx->stream>>>(a);
     PC_LAUNCHED(ctx, "match");
     return PC_OK;
 }
 
 template <int K, int NT>
-int launch_match_k(pc_ctx *ctx, const MatchArgs &a, size_t smem, int grid) {
-    switch (a.nb) {
-        case 1: return launch_match_t<1, K, NT>(ctx, a, smem, grid);
-        case 2: return launch_match_t<2, K, NT>(ctx, a, smem, grid);
-        case 3: return launch_match_t<3, K, NT>(ctx, a, smem, grid);
-        case 4: return launch_match_t<4, K, NT>(ctx, a, smem, grid);
-        case 5: return launch_match_t<5, K, NT>(ctx, a, smem, grid);
-        case 6: return launch_match_t<6, K, NT>(ctx, a, smem, grid);
-        case 7: return launch_match_t<7, K, NT>(ctx, a, smem, grid);
-        case 8: return launch_match_t<8, K, NT>(ctx, a, smem, grid);
+int launch_match_k(pc_ctx *ctx, const MatchArgs &a, uint32_t nb, size_t smem, int grid, int mode) {
+    switch (nb) {
+        case 1: return launch_match_t<1, K, NT>(ctx, a, smem, grid, mode);
+        case 2: return launch_match_t<2, K, NT>(ctx, a, smem, grid, mode);
+        case 3: return launch_match_t<3, K, NT>(ctx, a, smem, grid, mode);
+        case 4: return launch_match_t<4, K, NT>(ctx, a, smem, grid, mode);
+        case 5: return launch_match_t<5, K, NT>(ctx, a, smem, grid, mode);
+        case 6: return launch_match_t<6, K, NT>(ctx, a, smem, grid, mode);
+        case 7: return launch_match_t<7, K, NT>(ctx, a, smem, grid, mode);
+        case 8: return launch_match_t<8, K, NT>(ctx, a, smem, grid, mode);
     }
     return pc_fail(ctx, PC_INVALID, "unsupported bitset filter count");
 }
 
 template <int NT>
-int launch_match_n(pc_ctx *ctx, const MatchArgs &a, uint32_t K, size_t smem, int grid) {
-    if (K == 16) return launch_match_k<16, NT>(ctx, a, smem, grid);
-    if (K == 32) return launch_match_k<32, NT>(ctx, a, smem, grid);
-    return launch_match_k<64, NT>(ctx, a, smem, grid);
+int launch_match_n(pc_ctx *ctx, const MatchArgs &a, uint32_t nb, uint32_t K, size_t smem, int grid, int mode) {
+    if (K == 16) return launch_match_k<16, NT>(ctx, a, nb, smem, grid, mode);
+    if (K == 32) return launch_match_k<32, NT>(ctx, a, nb, smem, grid, mode);
+    return launch_match_k<64, NT>(ctx, a, nb, smem, grid, mode);
 }
 
 uint32_t inv_mod(uint32_t a, uint32_t q) {
@@ -829,9 +914,11 @@ extern "C" int pc_filters_create(pc_ctx *ctx, uint64_t A, uint64_t B, const uint
         return pc_fail(ctx, PC_INVALID, "first residual filters too large for bitset rows");
     }
     f->fc_bytes = nres * sizeof(FiltConst);
+    f->fcs_bytes = nres * sizeof(FiltC);
     f->bits_bytes = bits.size() * 4;
     f->pat_bytes = pat.size() * 4;
     int rc = pc_alloc(ctx, (void **)&f->d_fc, f->fc_bytes);
+    if (!rc) rc = pc_alloc(ctx, (void **)&f->d_fcs, f->fcs_bytes);
     if (!rc) rc = pc_alloc(ctx, (void **)&f->d_bits, f->bits_bytes);
     if (!rc) rc = pc_alloc(ctx, (void **)&f->d_pat, f->pat_bytes);
     if (rc) {
@@ -839,6 +926,7 @@ extern "C" int pc_filters_create(pc_ctx *ctx, uint64_t A, uint64_t B, const uint
         return rc;
     }
     cudaMemcpyAsync(f->d_fc, fc.data(), f->fc_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(f->d_fcs, f->fcs.data(), f->fcs_bytes, cudaMemcpyHostToDevice, ctx->stream);
     cudaMemcpyAsync(f->d_bits, bits.data(), f->bits_bytes, cudaMemcpyHostToDevice, ctx->stream);
     cudaMemcpyAsync(f->d_pat, pat.data(), f->pat_bytes, cudaMemcpyHostToDevice, ctx->stream);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
@@ -853,11 +941,13 @@ extern "C" int pc_filters_create(pc_ctx *ctx, uint64_t A, uint64_t B, const uint
 extern "C" int pc_filters_free(pc_ctx *ctx, pc_filters *f) {
     if (!f) return PC_OK;
     pc_release(ctx, f->d_fc, f->fc_bytes);
+    pc_release(ctx, f->d_fcs, f->fcs_bytes);
     pc_release(ctx, f->d_bits, f->bits_bytes);
     pc_release(ctx, f->d_pat, f->pat_bytes);
     delete f;
     return PC_OK;
 }
+
 
 namespace {
 
@@ -873,11 +963,22 @@ uint32_t cheap_count(const pc_filters *f, uint32_t nb) {
     return n;
 }
 
-Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_t *smem_out, uint32_t *tmax_out) {
-    Tuned r{};
-    uint32_t nb_min = std::min<uint32_t>(f->nres, 4);
-    r.nb = t && t->bitset_filters ? t->bitset_filters : std::min<uint32_t>(f->nbmax, 7);
-    r.nb = std::max(nb_min, std::min(r.nb, f->nbmax));
+// One launch shape for every family of a launch: NB inside every family's bitset range, the cheap
+// tier as deep as the shallowest family allows, shared memory sized by the largest rows and
+// counters.  Defaults: seven bitset filters, 32-word blocks, 1024 threads, stepping down (threads,
+// then block words, then bitset filters) until the layout fits the opt-in shared memory.
+int resolve_tuning(pc_ctx *ctx, const std::vector<const pc_filters *> &fams, const pc_tuning *t, Tuned &r,
+                   size_t &smem, uint32_t &tmax) {
+    uint32_t nb_lo = 1, nb_hi = PC_MAX_BITSET, ngmax = 0;
+    for (const pc_filters *f : fams) {
+        nb_lo = std::max(nb_lo, std::min<uint32_t>(f->nres, 4));
+        nb_hi = std::min(nb_hi, f->nbmax);
+        ngmax = std::max(ngmax, f->ng);
+    }
+    if (nb_lo > nb_hi) return pc_fail(ctx, PC_INVALID, "filter families cannot share one bitset launch");
+    r = Tuned{};
+    r.nb = t && t->bitset_filters ? t->bitset_filters : std::min<uint32_t>(nb_hi, 7);
+    r.nb = std::max(nb_lo, std::min(r.nb, nb_hi));
     r.K = t && t->block_words ? t->block_words : 32;
     if (r.K != 16 && r.K != 32 && r.K != 64) r.K = 32;
     const bool fixed_threads = t && t->threads;
@@ -888,248 +989,351 @@ Tuned resolve_tuning(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t, size_
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
     if (optin <= 0) optin = 227 * 1024;
     for (;;) {
-        r.nch = cheap_count(f, r.nb);
-        for (uint32_t tmax = TMAX_DEFAULT; tmax >= 4; tmax /= 2) {
-            MatchSmem L(f->rows_sum[r.nb], r.K, r.nb, r.nch, tmax, f->ng, r.threads / 32);
+        r.nch = PC_MAX_CHEAP;
+        uint32_t rows = 0;
+        for (const pc_filters *f : fams) {
+            r.nch = std::min(r.nch, cheap_count(f, r.nb));
+            rows = std::max(rows, f->rows_sum[r.nb]);
+        }
+        for (uint32_t tm = TMAX_DEFAULT; tm >= 4; tm /= 2) {
+            MatchSmem L(rows, r.K, r.nb, r.nch, tm, ngmax, r.threads / 32);
             if (L.total <= (uint32_t)optin) {
-                *tmax_out = tmax;
-                *smem_out = L.total;
-                return r;
+                tmax = tm;
+                smem = L.total;
+                return PC_OK;
             }
         }
         if (!fixed_threads && r.threads > 512) r.threads = r.threads == 1024 ? 768 : 512;
         else if (r.K > 16) r.K /= 2;
-        else if (r.nb > nb_min) r.nb--;
-        else {
-            *smem_out = 0;
-            return r;
-        }
+        else if (r.nb > nb_lo) r.nb--;
+        else return pc_fail(ctx, PC_INVALID, "residual rows do not fit shared memory");
     }
 }
 
-struct BatchIO {
-    uint64_t *counts, *geometry, *out;
-    uint64_t out_cap, *n_out;
-    pc_stats *stats;
+FamDev fam_dev(const pc_filters *f, uint32_t nb, uint32_t nch) {
+    FamDev d{};
+    d.nres = f->nres;
+    d.ng = f->ng;
+    d.total_rows = f->rows_sum[nb];
+    d.c2_live = nb == 8 || (nb > 4 && nb == f->nres);
+    for (uint32_t i = 0; i < nb; ++i) {
+        d.q[i] = f->primes[i];
+        d.row0[i] = f->rows_sum[i];
+        d.ainvb[i] = f->ainvb[i];
+        d.mq[i] = make_modq(f->primes[i]);
+    }
+    for (uint32_t t = 0; t < nch; ++t) {
+        const uint32_t q = f->primes[nb + t];
+        d.cq[t] = q;
+        d.caq[t] = (uint32_t)(f->A % q);
+        d.cbq[t] = (uint32_t)(f->B % q);
+        d.cmq[t] = make_modq(q);
+        d.cbits_off[t] = f->fcs[nb + t].tab_off;
+    }
+    for (uint32_t idx = 0; idx < 16; ++idx)
+        d.bgroup[idx] = (uint8_t)(idx < f->nres && ((idx & 3) == 3 || idx + 1 == f->nres) ? idx / 4 + 1 : 0);
+    d.pat = f->d_pat;
+    d.bits = f->d_bits;
+    d.fcs = f->d_fcs;
+    return d;
+}
+
+// The device half of stages 2 and 3 over a set of segments whose u and v lists are already on
+// the device.  Every buffer is sized once by engine_prepare, so the launch sequence (front + back)
+// can be recorded into a CUDA graph and replayed.
+struct Engine {
+    pc_ctx *ctx = nullptr;
+    const uint64_t *us = nullptr, *vs = nullptr;
+    uint64_t nu = 0, nv = 0;
+    std::vector<SegDev> segs;
+    std::vector<const pc_filters *> fams;
+    std::vector<FamDev> famdev;
+    std::vector<uint32_t> tile_seg;
+    uint64_t ntiles = 0, out_cap = 0;
+    Tuned tn{};
+    size_t smem = 0;
+    uint32_t tmax = 0, stride = 0, ngmax = 0;
+    uint64_t nblocks = 0;
+    int grid = 0;
+    uint32_t deep_cap = 1u << 15, deep_max = 0;
+    SegDev *d_seg = nullptr;
+    FamDev *d_fam = nullptr;
+    uint32_t *d_tile_seg = nullptr, *d_blk_seg = nullptr, *d_deep_count = nullptr;
+    uint64_t *d_counts = nullptr, *d_geo = nullptr, *d_out = nullptr;
+    unsigned long long *d_nout = nullptr;                 // [0] outputs, [1] rows outside the geometry
+    VRec *d_rec = nullptr;
+    uint4 *d_bv = nullptr;
+    uint64_t *d_pieces = nullptr, *d_tmp = nullptr, *d_items = nullptr, *d_prefix = nullptr, *d_vchunk = nullptr;
+    uint64_t *d_ws = nullptr;
+    uint4 *d_deep = nullptr;
+    uint64_t deep_bytes = 0;
+    ~Engine() {
+        if (ctx && d_deep) pc_release(ctx, d_deep, deep_bytes);
+    }
 };
 
-// Device part shared by pc_run_batch and pc_run_lease.
-int run_device(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const uint64_t *d_us, uint64_t nu,
-               const uint64_t *d_vs, uint64_t nv, u128 lo, u128 hi, uint64_t v_first, uint64_t width,
-               uint32_t ntiles, uint64_t v_end, const BatchIO &io, int launches0) {
-    if (nu >= (UINT64_C(1) << 31) || nv >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "focus list too long");
-    if (hi.hi >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "interval bound must be below 2^96");
-    if (f->nres > (uint32_t)FC_INLINE) return pc_fail(ctx, PC_INVALID, "more residual filters than the fused kernel holds");
-    const uint32_t ng = f->ng, stride = ng + 3;
-    size_t smem = 0;
-    uint32_t tmax = 0;
-    Tuned tn = resolve_tuning(ctx, f, tuning, &smem, &tmax);
-    if (!smem) return pc_fail(ctx, PC_INVALID, "residual rows do not fit shared memory");
-    const int grid = ctx->sm_count;
-    uint32_t deep_cap = 1u << 15;
-    for (int attempt = 0;; ++attempt) {
-        Scratch s(ctx);
-        uint64_t *d_counts, *d_geo, *d_out, *d_prefix, *d_vchunk, *d_pieces;
-        unsigned long long *d_nout, *d_bad;
-        VRec *d_rec;
-        uint4 *d_bv, *d_deep;
-        uint32_t *d_deep_count;
-        const uint32_t UB = tn.K * 32;
-        const uint64_t nblocks = (nu + UB - 1) / UB;
-        int rc = s.get(&d_counts, (uint64_t)ntiles * stride);
-        if (!rc) rc = s.get(&d_geo, 2 * (uint64_t)ntiles);
-        if (!rc) rc = s.get(&d_out, 2 * std::max<uint64_t>(1, io.out_cap));
-        if (!rc) rc = s.get(&d_nout, 2);
-        if (!rc) rc = s.get(&d_rec, std::max<uint64_t>(1, nv));
-        if (!rc) rc = s.get(&d_bv, std::max<uint64_t>(1, nblocks));
-        if (!rc) rc = s.get(&d_pieces, std::max<uint64_t>(1, nblocks));
-        if (!rc) rc = s.get(&d_prefix, nblocks + 1);
-        if (!rc) rc = s.get(&d_vchunk, 1);
-        if (!rc) rc = s.get(&d_deep, (uint64_t)grid * deep_cap);
-        if (!rc) rc = s.get(&d_deep_count, grid);
-        if (rc) return rc;
-        d_bad = d_nout + 1;
-        cudaStream_t st = ctx->stream;
-        PC_CHECK(ctx, cudaMemsetAsync(d_counts, 0, (uint64_t)ntiles * stride * 8, st));
-        PC_CHECK(ctx, cudaMemsetAsync(d_nout, 0, 16, st));
-        PC_CHECK(ctx, cudaMemsetAsync(d_deep_count, 0, (uint64_t)grid * 4, st));
-        PC_CHECK(ctx, cudaEventRecord(ctx->ev[0], st));
-        int launches = launches0;
+int engine_deep_alloc(Engine &E, uint32_t cap) {
+    if (E.d_deep) pc_release(E.ctx, E.d_deep, E.deep_bytes);
+    E.d_deep = nullptr;
+    E.deep_cap = cap;
+    E.deep_bytes = (uint64_t)E.grid * cap * sizeof(uint4);
+    return pc_alloc(E.ctx, (void **)&E.d_deep, E.deep_bytes);
+}
 
+int engine_prepare(Engine &E, const pc_tuning *tuning, Scratch &hold) {
+    pc_ctx *ctx = E.ctx;
+    if (E.nu >= (UINT64_C(1) << 31) || E.nv >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "focus list too long");
+    if (E.segs.empty() || E.fams.empty()) return pc_fail(ctx, PC_INVALID, "no segments");
+    for (const SegDev &g : E.segs)
+        if (g.hi.hi >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "interval bound must be below 2^96");
+    int rc = resolve_tuning(ctx, E.fams, tuning, E.tn, E.smem, E.tmax);
+    if (rc) return rc;
+    E.ngmax = 0;
+    for (const pc_filters *f : E.fams) E.ngmax = std::max(E.ngmax, f->ng);
+    E.stride = E.ngmax + 3;
+    E.famdev.clear();
+    for (const pc_filters *f : E.fams) E.famdev.push_back(fam_dev(f, E.tn.nb, E.tn.nch));
+    E.grid = ctx->sm_count;
+    if (tuning && tuning->deep_records) E.deep_cap = tuning->deep_records;
+    const uint32_t UB = E.tn.K * 32;
+    E.nblocks = (E.nu + UB - 1) / UB;
+    const uint64_t nb1 = std::max<uint64_t>(1, E.nblocks);
+    rc = hold.get(&E.d_seg, E.segs.size());
+    if (!rc) rc = hold.get(&E.d_fam, E.famdev.size());
+    if (!rc) rc = hold.get(&E.d_tile_seg, std::max<uint64_t>(1, E.ntiles));
+    if (!rc) rc = hold.get(&E.d_counts, std::max<uint64_t>(1, E.ntiles * E.stride));
+    if (!rc) rc = hold.get(&E.d_geo, std::max<uint64_t>(1, 2 * E.ntiles));
+    if (!rc) rc = hold.get(&E.d_out, 2 * std::max<uint64_t>(1, E.out_cap));
+    if (!rc) rc = hold.get(&E.d_nout, 2);
+    if (!rc) rc = hold.get(&E.d_rec, std::max<uint64_t>(1, E.nv));
+    if (!rc) rc = hold.get(&E.d_bv, nb1);
+    if (!rc) rc = hold.get(&E.d_blk_seg, nb1);
+    if (!rc) rc = hold.get(&E.d_pieces, nb1);
+    if (!rc) rc = hold.get(&E.d_tmp, E.nblocks + 1);
+    if (!rc) rc = hold.get(&E.d_items, nb1);
+    if (!rc) rc = hold.get(&E.d_prefix, E.nblocks + 1);
+    if (!rc) rc = hold.get(&E.d_vchunk, 1);
+    if (!rc) rc = hold.get(&E.d_ws, pc_scan_workspace(E.nblocks));
+    if (!rc) rc = hold.get(&E.d_deep_count, E.grid);
+    if (!rc) rc = engine_deep_alloc(E, E.deep_cap);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    PC_CHECK(ctx, cudaMemcpyAsync(E.d_seg, E.segs.data(), E.segs.size() * sizeof(SegDev), cudaMemcpyHostToDevice, st));
+    PC_CHECK(ctx, cudaMemcpyAsync(E.d_fam, E.famdev.data(), E.famdev.size() * sizeof(FamDev), cudaMemcpyHostToDevice, st));
+    if (E.ntiles)
+        PC_CHECK(ctx, cudaMemcpyAsync(E.d_tile_seg, E.tile_seg.data(), E.ntiles * 4, cudaMemcpyHostToDevice, st));
+    return PC_OK;
+}
+
+// mode 0: set the shared-memory attribute and launch; 1: launch only (inside a capture);
+// 2: set the attribute only.
+int engine_match(Engine &E, int mode) {
+    MatchArgs ma{};
+    ma.us = E.us;
+    ma.rec = E.d_rec;
+    ma.seg = E.d_seg;
+    ma.fam = E.d_fam;
+    ma.blk_seg = E.d_blk_seg;
+    ma.nch = E.tn.nch;
+    ma.tmax = E.tmax;
+    ma.stride = E.stride;
+    ma.total_rows = 0;
+    for (const FamDev &d : E.famdev) ma.total_rows = std::max(ma.total_rows, d.total_rows);
+    ma.counts = E.d_counts;
+    ma.bv = E.d_bv;
+    ma.item_prefix = E.d_prefix;
+    ma.nblocks = E.nblocks;
+    ma.vchunk = E.d_vchunk;
+    ma.deep = E.d_deep;
+    ma.deep_cap = E.deep_cap;
+    ma.deep_count = E.d_deep_count;
+    if (E.tn.threads == 1024) return launch_match_n<1024>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
+    if (E.tn.threads == 768) return launch_match_n<768>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
+    return launch_match_n<512>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
+}
+
+// Counters reset, per-v bounds, subtile envelopes, block ranges, work items and the fused match.
+int engine_front(Engine &E, bool events, bool capturing, int *launches) {
+    pc_ctx *ctx = E.ctx;
+    cudaStream_t st = ctx->stream;
+    if (E.ntiles) PC_CHECK(ctx, cudaMemsetAsync(E.d_counts, 0, E.ntiles * E.stride * 8, st));
+    PC_CHECK(ctx, cudaMemsetAsync(E.d_nout, 0, 16, st));
+    PC_CHECK(ctx, cudaMemsetAsync(E.d_deep_count, 0, (uint64_t)E.grid * 4, st));
+    if (events) PC_CHECK(ctx, cudaEventRecord(ctx->ev[0], st));
+    if (E.nv) {
         PrepArgs pa{};
-        pa.us = d_us;
-        pa.vs = d_vs;
-        pa.nu = nu;
-        pa.nv = nv;
-        pa.A = f->A;
-        pa.B = f->B;
-        pa.lo = lo;
-        pa.hi = hi;
-        pa.v_first = v_first;
-        pa.width = width;
-        pa.ntiles = ntiles;
-        pa.nb = tn.nb;
-        pa.ng = ng;
-        for (uint32_t i = 0; i < tn.nb; ++i) {
-            pa.q[i] = f->primes[i];
-            pa.row0[i] = f->rows_sum[i];
-            pa.mq[i] = make_modq(f->primes[i]);
-        }
-        pa.rec = d_rec;
-        pa.counts = d_counts;
-        pa.bad = d_bad;
-        if (nv) {
-            uint64_t runs = (nv + PREP_RUN - 1) / PREP_RUN;
-            k_vprep<<<(unsigned)((runs + 127) / 128), 128, 0, st>>>(pa);
-            PC_LAUNCHED(ctx, "vprep");
-            ++launches;
-        }
-        k_geometry<<<(ntiles + 127) / 128, 128, 0, st>>>(d_us, nu, d_vs, nv, f->A, f->B, lo, hi, v_first, width,
-                                                          v_end, ntiles, d_geo);
-        PC_LAUNCHED(ctx, "geometry");
-        ++launches;
-        PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], st));
-        const bool run_match = nu && nv;
-        uint32_t deep_max = 0;
-        if (run_match) {
-            k_blocks<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_rec, nv, nu, UB, nblocks, d_bv, d_pieces);
-            PC_LAUNCHED(ctx, "blocks");
-            uint64_t *d_items, *d_tmp;
-            rc = s.get(&d_items, nblocks);
-            if (!rc) rc = s.get(&d_tmp, nblocks + 1);
-            if (!rc) rc = pc_exclusive_scan_u64(ctx, d_pieces, d_tmp, nblocks, d_tmp + nblocks);
-            if (rc) return rc;
-            k_chunk<<<1, 1, 0, st>>>(d_tmp + nblocks, tn.v_chunk, (uint64_t)grid * 32, d_vchunk);
-            PC_LAUNCHED(ctx, "chunk");
-            k_item_counts<<<(unsigned)((nblocks + 255) / 256), 256, 0, st>>>(d_pieces, nblocks, d_vchunk, d_items);
-            PC_LAUNCHED(ctx, "item counts");
-            rc = pc_exclusive_scan_u64(ctx, d_items, d_prefix, nblocks, d_prefix + nblocks);
-            if (rc) return rc;
-            launches += 7;
-            MatchArgs ma{};
-            ma.us = d_us;
-            ma.vs = d_vs;
-            ma.rec = d_rec;
-            ma.nu = nu;
-            ma.nv = nv;
-            ma.A = f->A;
-            ma.B = f->B;
-            ma.lo = lo;
-            ma.hi = hi;
-            ma.nres = f->nres;
-            ma.ng = ng;
-            ma.nb = tn.nb;
-            ma.tmax = tmax;
-            ma.fc = f->d_fc;
-            ma.bits = f->d_bits;
-            ma.pat = f->d_pat;
-            for (uint32_t i = 0; i < tn.nb; ++i) {
-                ma.q[i] = f->primes[i];
-                ma.row0[i] = f->rows_sum[i];
-                ma.ainvb[i] = f->ainvb[i];
-                ma.mq[i] = make_modq(f->primes[i]);
-            }
-            ma.total_rows = f->rows_sum[tn.nb];
-            ma.counts = d_counts;
-            ma.out = d_out;
-            ma.out_cap = io.out_cap;
-            ma.n_out = d_nout;
-            ma.ntiles = ntiles;
-            ma.bv = d_bv;
-            ma.item_prefix = d_prefix;
-            ma.nblocks = nblocks;
-            ma.vchunk = d_vchunk;
-            ma.v_first = v_first;
-            ma.width = width;
-            ma.nch = tn.nch;
-            for (uint32_t t = 0; t < tn.nch; ++t) {
-                const uint32_t q = f->primes[tn.nb + t];
-                ma.cq[t] = q;
-                ma.caq[t] = (uint32_t)(f->A % q);
-                ma.cbq[t] = (uint32_t)(f->B % q);
-                ma.cmq[t] = make_modq(q);
-                ma.cbits_off[t] = f->fcs[tn.nb + t].tab_off;
-            }
-            for (uint32_t idx = 0; idx < 16; ++idx)
-                ma.bgroup[idx] = (uint8_t)(idx < f->nres && ((idx & 3) == 3 || idx + 1 == f->nres) ? idx / 4 + 1 : 0);
-            ma.deep = d_deep;
-            ma.deep_cap = deep_cap;
-            ma.deep_count = d_deep_count;
-            PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
-            if (tn.threads == 1024) rc = launch_match_n<1024>(ctx, ma, tn.K, smem, grid);
-            else if (tn.threads == 768) rc = launch_match_n<768>(ctx, ma, tn.K, smem, grid);
-            else rc = launch_match_n<512>(ctx, ma, tn.K, smem, grid);
-            if (rc) return rc;
-            ++launches;
-            std::vector<uint32_t> deep_counts(grid);
-            PC_CHECK(ctx, cudaMemcpyAsync(deep_counts.data(), d_deep_count, (uint64_t)grid * 4, cudaMemcpyDeviceToHost, st));
-            PC_CHECK(ctx, cudaStreamSynchronize(st));
-            for (uint32_t c : deep_counts) deep_max = std::max(deep_max, c);
-            if (deep_max > deep_cap) {
-                if (attempt) return pc_fail(ctx, PC_ARITHMETIC, "deep survivor count changed between attempts");
-                deep_cap = deep_max + 1024;
-                continue;                                  // rerun with room for every deep survivor
-            }
-            DeepArgs da{};
-            da.us = d_us;
-            da.deep = d_deep;
-            da.deep_count = d_deep_count;
-            da.deep_cap = deep_cap;
-            da.slices = grid;
-            da.A = f->A;
-            da.B = f->B;
-            da.first = tn.nb + tn.nch;
-            da.nres = f->nres;
-            da.ng = ng;
-            da.ntiles = ntiles;
-            da.bits = f->d_bits;
-            da.counts = d_counts;
-            da.out = d_out;
-            da.out_cap = io.out_cap;
-            da.n_out = d_nout;
-            for (uint32_t i = 0; i < f->nres && i < (uint32_t)FC_INLINE; ++i) da.fcs[i] = f->fcs[i];
-            if (deep_max) {
-                dim3 dg((unsigned)std::min<uint64_t>((deep_max + 255) / 256, 64), (unsigned)grid);
-                k_deep<<<dg, 256, 0, st>>>(da);
-                PC_LAUNCHED(ctx, "deep");
-                ++launches;
-            }
-            PC_CHECK(ctx, cudaEventRecord(ctx->ev[3], st));
-        }
-        unsigned long long host_nout[2] = {0, 0};
-        PC_CHECK(ctx, cudaMemcpyAsync(host_nout, d_nout, 16, cudaMemcpyDeviceToHost, st));
-        PC_CHECK(ctx, cudaMemcpyAsync(io.counts, d_counts, (uint64_t)ntiles * stride * 8, cudaMemcpyDeviceToHost, st));
-        PC_CHECK(ctx, cudaMemcpyAsync(io.geometry, d_geo, 2 * (uint64_t)ntiles * 8, cudaMemcpyDeviceToHost, st));
-        PC_CHECK(ctx, cudaStreamSynchronize(st));
-        uint64_t n = host_nout[0];
-        *io.n_out = n;
-        if (io.stats) {
-            io.stats->bounds_ms = elapsed_ms(ctx->ev[0], ctx->ev[1]);
-            io.stats->kernel_ms = run_match ? elapsed_ms(ctx->ev[2], ctx->ev[3]) : 0.0;
-            io.stats->outputs = n;
-            io.stats->launches = launches;
-            io.stats->work_items = deep_max;
-            io.stats->reserved[0] = tn.nb;
-            io.stats->reserved[1] = tn.K;
-            io.stats->reserved[2] = tn.threads;
-            io.stats->reserved[3] = tn.nch;
-        }
-        if (host_nout[1]) return pc_fail(ctx, PC_INVALID, "v row outside the subtile geometry");
-        if (n > io.out_cap) return pc_fail(ctx, PC_OVERFLOW, "output overflow; attempt cannot commit");
-        if (n) {
-            PC_CHECK(ctx, cudaMemcpyAsync(io.out, d_out, 2 * n * 8, cudaMemcpyDeviceToHost, st));
-            PC_CHECK(ctx, cudaStreamSynchronize(st));
-        }
-        for (uint32_t t = 0; t < ntiles; ++t)
-            if (io.counts[(uint64_t)t * stride + ng + 2]) return pc_fail(ctx, PC_ARITHMETIC, "unsigned underflow flagged");
-        return PC_OK;
+        pa.us = E.us;
+        pa.vs = E.vs;
+        pa.nv = E.nv;
+        pa.seg = E.d_seg;
+        pa.nseg = (uint32_t)E.segs.size();
+        pa.fam = E.d_fam;
+        pa.nb = E.tn.nb;
+        pa.stride = E.stride;
+        pa.rec = E.d_rec;
+        pa.counts = E.d_counts;
+        pa.bad = E.d_nout + 1;
+        const uint64_t runs = (E.nv + PREP_RUN - 1) / PREP_RUN;
+        k_vprep<<<(unsigned)((runs + 127) / 128), 128, 0, st>>>(pa);
+        PC_LAUNCHED(ctx, "vprep");
+        ++*launches;
     }
+    if (E.ntiles) {
+        k_geometry<<<(unsigned)((E.ntiles + 127) / 128), 128, 0, st>>>(E.us, E.vs, E.d_seg, E.d_tile_seg, E.ntiles, E.d_geo);
+        PC_LAUNCHED(ctx, "geometry");
+        ++*launches;
+    }
+    if (events) PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], st));
+    if (!E.nu || !E.nv) return PC_OK;
+    const uint32_t UB = E.tn.K * 32;
+    k_blocks<<<(unsigned)((E.nblocks + 255) / 256), 256, 0, st>>>(E.d_rec, E.d_seg, (uint32_t)E.segs.size(), UB,
+                                                                 E.nblocks, E.d_bv, E.d_blk_seg, E.d_pieces);
+    PC_LAUNCHED(ctx, "blocks");
+    int rc = pc_exclusive_scan_ws(ctx, E.d_pieces, E.d_tmp, E.nblocks, E.d_tmp + E.nblocks, E.d_ws);
+    if (rc) return rc;
+    k_chunk<<<1, 1, 0, st>>>(E.d_tmp + E.nblocks, E.tn.v_chunk, (uint64_t)E.grid * 32, E.d_vchunk);
+    PC_LAUNCHED(ctx, "chunk");
+    k_item_counts<<<(unsigned)((E.nblocks + 255) / 256), 256, 0, st>>>(E.d_pieces, E.nblocks, E.d_vchunk, E.d_items);
+    PC_LAUNCHED(ctx, "item counts");
+    rc = pc_exclusive_scan_ws(ctx, E.d_items, E.d_prefix, E.nblocks, E.d_prefix + E.nblocks, E.d_ws);
+    if (rc) return rc;
+    *launches += 7;
+    if (events) PC_CHECK(ctx, cudaEventRecord(ctx->ev[2], st));
+    rc = engine_match(E, capturing ? 1 : 0);
+    if (rc) return rc;
+    ++*launches;
+    return PC_OK;
+}
+
+// The exact later filters on the deep survivors.
+int engine_back(Engine &E, bool events, int *launches) {
+    pc_ctx *ctx = E.ctx;
+    if (E.nu && E.nv && E.deep_max) {
+        DeepArgs da{};
+        da.us = E.us;
+        da.deep = E.d_deep;
+        da.deep_count = E.d_deep_count;
+        da.deep_cap = E.deep_cap;
+        da.first = E.tn.nb + E.tn.nch;
+        da.stride = E.stride;
+        da.ntiles = E.ntiles;
+        da.seg = E.d_seg;
+        da.fam = E.d_fam;
+        da.tile_seg = E.d_tile_seg;
+        da.counts = E.d_counts;
+        da.out = E.d_out;
+        da.out_cap = E.out_cap;
+        da.n_out = E.d_nout;
+        dim3 dg((unsigned)std::min<uint64_t>((E.deep_max + 255) / 256, 64), (unsigned)E.grid);
+        k_deep<<<dg, 256, 0, ctx->stream>>>(da);
+        PC_LAUNCHED(ctx, "deep");
+        ++*launches;
+    }
+    if (events) PC_CHECK(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+    return PC_OK;
+}
+
+// Eager run: the match, the deep-survivor counts on the host (a rerun with room for every deep
+// survivor when a slice overflowed), then the deep tier.
+int engine_eager(Engine &E, int *launches) {
+    pc_ctx *ctx = E.ctx;
+    for (int attempt = 0;; ++attempt) {
+        int rc = engine_front(E, true, false, launches);
+        if (rc) return rc;
+        E.deep_max = 0;
+        if (E.nu && E.nv) {
+            std::vector<uint32_t> deep_counts(E.grid);
+            PC_CHECK(ctx, cudaMemcpyAsync(deep_counts.data(), E.d_deep_count, (uint64_t)E.grid * 4, cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+            PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+            for (uint32_t c : deep_counts) E.deep_max = std::max(E.deep_max, c);
+            if (E.deep_max > E.deep_cap) {
+                if (attempt) return pc_fail(ctx, PC_ARITHMETIC, "deep survivor count changed between attempts");
+                rc = engine_deep_alloc(E, E.deep_max + 1024);
+                if (rc) return rc;
+                continue;
+            }
+        }
+        return engine_back(E, true, launches);
+    }
+}
+
+// Results of a finished run already copied to the host: output count, rows outside the subtile
+// geometry, and the underflow counters of every subtile.
+int engine_check(Engine &E, const unsigned long long nout[2], const uint64_t *counts) {
+    if (nout[1]) return pc_fail(E.ctx, PC_INVALID, "v row outside the subtile geometry");
+    if (nout[0] > E.out_cap) return pc_fail(E.ctx, PC_OVERFLOW, "output overflow; attempt cannot commit");
+    for (uint64_t t = 0; t < E.ntiles; ++t) {
+        const uint32_t ng = E.fams[E.segs[E.tile_seg[t]].fam]->ng;
+        if (counts[t * E.stride + ng + 2]) return pc_fail(E.ctx, PC_ARITHMETIC, "unsigned underflow flagged");
+    }
+    return PC_OK;
+}
+
+int engine_collect(Engine &E, uint64_t *counts, uint64_t *geometry, uint64_t *out, uint64_t *n_out) {
+    pc_ctx *ctx = E.ctx;
+    cudaStream_t st = ctx->stream;
+    unsigned long long nout[2] = {0, 0};
+    PC_CHECK(ctx, cudaMemcpyAsync(nout, E.d_nout, 16, cudaMemcpyDeviceToHost, st));
+    if (E.ntiles) {
+        PC_CHECK(ctx, cudaMemcpyAsync(counts, E.d_counts, E.ntiles * E.stride * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, cudaMemcpyAsync(geometry, E.d_geo, 2 * E.ntiles * 8, cudaMemcpyDeviceToHost, st));
+    }
+    PC_CHECK(ctx, cudaStreamSynchronize(st));
+    *n_out = nout[0];
+    int rc = engine_check(E, nout, counts);
+    if (rc) return rc;
+    if (nout[0]) {
+        PC_CHECK(ctx, cudaMemcpyAsync(out, E.d_out, 2 * nout[0] * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, cudaStreamSynchronize(st));
+    }
+    return PC_OK;
+}
+
+void engine_stats(Engine &E, pc_stats *stats, int launches, uint64_t n_out) {
+    if (!stats) return;
+    pc_ctx *ctx = E.ctx;
+    const bool matched = E.nu && E.nv;
+    stats->bounds_ms = elapsed_ms(ctx->ev[0], ctx->ev[1]);
+    stats->kernel_ms = matched ? elapsed_ms(ctx->ev[2], ctx->ev[3]) : 0.0;
+    stats->outputs = n_out;
+    stats->launches = launches;
+    stats->work_items = E.deep_max;
+    stats->reserved[0] = E.tn.nb;
+    stats->reserved[1] = E.tn.K;
+    stats->reserved[2] = E.tn.threads;
+    stats->reserved[3] = E.tn.nch;
+}
+
+// True when ntiles subtiles of width v fit below 2^64 and match the [first, end) span.
+bool tiles_fit(uint64_t first, uint64_t end, uint64_t width, uint64_t ntiles) {
+    typedef unsigned __int128 w128;
+    if (!width || end <= first) return false;
+    if (((w128)ntiles * width) >> 64) return false;
+    return (end - first + width - 1) / width == ntiles;
+}
+
+SegDev one_segment(const pc_filters *f, uint64_t nu, uint64_t nv, u128 lo, u128 hi, uint64_t v_first,
+                   uint64_t width, uint64_t v_end, uint32_t ntiles) {
+    SegDev g{};
+    g.A = f->A;
+    g.B = f->B;
+    g.lo = lo;
+    g.hi = hi;
+    g.v_first = v_first;
+    g.width = width;
+    g.v_end = v_end;
+    g.u_off = 0;
+    g.nu = (uint32_t)nu;
+    g.v_off = 0;
+    g.nv = (uint32_t)nv;
+    g.tile_base = 0;
+    g.ntiles = ntiles;
+    g.fam = 0;
+    return g;
 }
 
 }  // namespace
-
-int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, uint64_t cap, uint64_t **out,
-                   uint64_t *out_bytes, uint64_t *total_host, int *launches);
 
 extern "C" int pc_run_batch(pc_ctx *ctx, const pc_filters *f, const pc_tuning *tuning, const pc_buf *us, uint64_t u_off,
                             uint64_t nu, const pc_buf *vs, uint64_t v_off, uint64_t nv, uint64_t lo0, uint64_t lo1,
@@ -1139,13 +1343,29 @@ extern "C" int pc_run_batch(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t
     if (!f || !us || !vs || width == 0 || ntiles == 0) return pc_fail(ctx, PC_INVALID, "invalid batch arguments");
     if (u_off > us->n || nu > us->n - u_off || v_off > vs->n || nv > vs->n - v_off)
         return pc_fail(ctx, PC_INVALID, "focus list slice out of range");
-    if (v_end <= v_first || (v_end - v_first + width - 1) / width != ntiles)
+    if (!tiles_fit(v_first, v_end, width, ntiles) || ntiles >= (UINT32_C(1) << 31))
         return pc_fail(ctx, PC_INVALID, "inconsistent subtile geometry");
     if (stats) memset(stats, 0, sizeof(*stats));
+    *n_out = 0;
     auto t0 = std::chrono::steady_clock::now();
-    BatchIO io{counts, geometry, out, out_cap, n_out, stats};
-    int rc = run_device(ctx, f, tuning, us->d + u_off, nu, vs->d + v_off, nv, u128{lo0, lo1}, u128{hi0, hi1}, v_first,
-                        width, ntiles, v_end, io, 0);
+    Engine E;
+    E.ctx = ctx;
+    E.us = us->d + u_off;
+    E.vs = vs->d + v_off;
+    E.nu = nu;
+    E.nv = nv;
+    if (nu >= (UINT64_C(1) << 31) || nv >= (UINT64_C(1) << 32)) return pc_fail(ctx, PC_INVALID, "focus list too long");
+    E.segs.push_back(one_segment(f, nu, nv, u128{lo0, lo1}, u128{hi0, hi1}, v_first, width, v_end, ntiles));
+    E.fams.push_back(f);
+    E.tile_seg.assign(ntiles, 0);
+    E.ntiles = ntiles;
+    E.out_cap = out_cap;
+    Scratch hold(ctx);
+    int launches = 0;
+    int rc = engine_prepare(E, tuning, hold);
+    if (!rc) rc = engine_eager(E, &launches);
+    if (!rc) rc = engine_collect(E, counts, geometry, out, n_out);
+    if (!rc || rc == PC_OVERFLOW || rc == PC_ARITHMETIC) engine_stats(E, stats, launches, *n_out);
     if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }
@@ -1156,28 +1376,46 @@ extern "C" int pc_run_lease(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb,
                             uint64_t *out, uint64_t out_cap, uint64_t *n_out, pc_stats *stats) {
     if (!fa || !fb || !f || width == 0 || end <= first) return pc_fail(ctx, PC_INVALID, "invalid lease arguments");
     if (stats) memset(stats, 0, sizeof(*stats));
+    *n_out = 0;
     auto t0 = std::chrono::steady_clock::now();
     typedef unsigned __int128 w128;
-    w128 lo = (w128)lo1 << 64 | lo0, hi = (w128)hi1 << 64 | hi0;
-    w128 ulo = (lo + (w128)first * f->A) / f->B + 1, uhi = (hi + (w128)(end - 1) * f->A) / f->B + 1;
+    const w128 lo = (w128)lo1 << 64 | lo0, hi = (w128)hi1 << 64 | hi0;
+    const w128 ulo = (lo + (w128)first * f->A) / f->B + 1, uhi = (hi + (w128)(end - 1) * f->A) / f->B + 1;
     if (uhi >> 64) return pc_fail(ctx, PC_INVALID, "u window exceeds 64 bits");
-    uint64_t ntiles64 = (end - first + width - 1) / width;
-    if (ntiles64 >= (UINT64_C(1) << 31)) return pc_fail(ctx, PC_INVALID, "too many subtiles");
+    const uint64_t ntiles64 = (end - first + width - 1) / width;
+    if (ntiles64 >= (UINT64_C(1) << 31) || !tiles_fit(first, end, width, ntiles64))
+        return pc_fail(ctx, PC_INVALID, "too many subtiles");
     int launches = 0;
+    Scratch hold(ctx);
     PC_CHECK(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
-    uint64_t *d_us = nullptr, *d_vs = nullptr, us_bytes = 0, vs_bytes = 0, nu = 0, nv = 0;
-    const uint64_t cap = (UINT64_C(1) << 32) - 1;
-    int rc = pc_window_into(ctx, fa, (uint64_t)ulo, (uint64_t)uhi, cap, &d_us, &us_bytes, &nu, &launches);
-    if (!rc) rc = pc_window_into(ctx, fb, first, end, cap, &d_vs, &vs_bytes, &nv, &launches);
-    if (!rc) {
-        cudaEventRecord(ctx->ev[5], ctx->stream);
-        BatchIO io{counts, geometry, out, out_cap, n_out, stats};
-        rc = run_device(ctx, f, tuning, d_us ? d_us : (const uint64_t *)nullptr, nu, d_vs, nv, u128{lo0, lo1},
-                        u128{hi0, hi1}, first, width, (uint32_t)ntiles64, end, io, launches);
+    const pc_focus *foc[2] = {fa, fb};
+    const uint64_t lows[2] = {(uint64_t)ulo, first}, highs[2] = {(uint64_t)uhi, end};
+    WinBatch wb;
+    int rc = winbatch_plan(ctx, hold, foc, lows, highs, nullptr, 2, (UINT64_C(1) << 32) - 1, wb, &launches);
+    uint64_t *d_lists = nullptr;
+    if (!rc) rc = hold.get(&d_lists, std::max<uint64_t>(1, wb.out_len));
+    if (!rc) rc = winbatch_emit(ctx, wb, d_lists);
+    if (rc) return rc;
+    ++launches;
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[5], ctx->stream));
+    Engine E;
+    E.ctx = ctx;
+    E.us = d_lists + wb.base[0];
+    E.nu = wb.total[0];
+    E.vs = d_lists + wb.base[1];
+    E.nv = wb.total[1];
+    E.segs.push_back(one_segment(f, E.nu, E.nv, u128{lo0, lo1}, u128{hi0, hi1}, first, width, end, (uint32_t)ntiles64));
+    E.fams.push_back(f);
+    E.tile_seg.assign(ntiles64, 0);
+    E.ntiles = ntiles64;
+    E.out_cap = out_cap;
+    rc = engine_prepare(E, tuning, hold);
+    if (!rc) rc = engine_eager(E, &launches);
+    if (!rc) rc = engine_collect(E, counts, geometry, out, n_out);
+    if (!rc || rc == PC_OVERFLOW || rc == PC_ARITHMETIC) {
+        engine_stats(E, stats, launches, *n_out);
         if (stats) stats->window_ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
     }
-    pc_release(ctx, d_us, us_bytes);
-    pc_release(ctx, d_vs, vs_bytes);
     if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }
@@ -1233,6 +1471,300 @@ extern "C" int pc_run_plain(pc_ctx *ctx, const pc_filters *f, const pc_buf *us, 
         PC_CHECK(ctx, cudaMemcpyAsync(out, d_out, 2 * copy * 8, cudaMemcpyDeviceToHost, st));
         PC_CHECK(ctx, cudaStreamSynchronize(st));
     }
+    return PC_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Many windows in one launch sequence (pc_multi_*).
+//
+// Every window carries its own interval, v range, subtile width, focus pair and filter family.
+// Creation plans all u windows (on each window's A focus) and v windows (on its B focus), sizes
+// every buffer and keeps them; a run regenerates the windows on the device and runs stages 2 and
+// 3 over all of them as segments of one launch sequence.  With PC_RUN_GRAPH the sequence after
+// the first eager run is recorded once into a CUDA graph and replayed.
+
+struct pc_multi {
+    pc_ctx *ctx;
+    Scratch hold;                        // device buffers kept for the object's lifetime
+    WinBatch wb;
+    uint64_t *d_lists = nullptr;         // u windows (each on a 2048-entry boundary), then v windows
+    Engine E;
+    uint32_t nwin = 0;
+    std::vector<uint32_t> tile_base;     // nwin + 1
+    std::vector<uint64_t> sizes;         // per window: u count, v count
+    std::vector<uint64_t> counts, geometry, out;
+    uint64_t n_out = 0;
+    int launches = 0;
+    bool ran = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t *h_counts = nullptr, *h_geo = nullptr;   // pinned copies written by the graph
+    unsigned long long *h_nout = nullptr;
+    uint32_t *h_deep = nullptr;
+    explicit pc_multi(pc_ctx *c) : ctx(c), hold(c) { E.ctx = c; }
+    ~pc_multi() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (h_counts) cudaFreeHost(h_counts);
+        if (h_geo) cudaFreeHost(h_geo);
+        if (h_nout) cudaFreeHost(h_nout);
+        if (h_deep) cudaFreeHost(h_deep);
+    }
+};
+
+extern "C" int pc_multi_create(pc_ctx *ctx, const pc_focus *const *foci, uint32_t nfoci,
+                               const pc_filters *const *families, uint32_t nfam, const pc_window *windows,
+                               uint32_t nwin, const pc_tuning *tuning, uint64_t out_cap, pc_multi **out) {
+    *out = nullptr;
+    if (!foci || !families || !windows || nwin == 0) return pc_fail(ctx, PC_INVALID, "invalid window batch arguments");
+    typedef unsigned __int128 w128;
+    std::vector<const pc_focus *> focs(2 * (size_t)nwin);
+    std::vector<uint64_t> lows(2 * (size_t)nwin), highs(2 * (size_t)nwin), pads(2 * (size_t)nwin);
+    std::vector<uint32_t> fam_map(nfam, UINT32_MAX), tile_base(nwin + 1, 0);
+    std::vector<const pc_filters *> used;
+    uint64_t ntiles = 0;
+    for (uint32_t i = 0; i < nwin; ++i) {
+        const pc_window &w = windows[i];
+        if (w.focus_a >= nfoci || w.focus_b >= nfoci || w.family >= nfam)
+            return pc_fail(ctx, PC_INVALID, "window refers to a missing focus or filter family");
+        const pc_filters *f = families[w.family];
+        const pc_focus *fa = foci[w.focus_a], *fb = foci[w.focus_b];
+        if (!f || !fa || !fb) return pc_fail(ctx, PC_INVALID, "null focus or filter family");
+        if (pc_focus_modulus(fa) != f->A || pc_focus_modulus(fb) != f->B)
+            return pc_fail(ctx, PC_INVALID, "focus moduli differ from the filter family's A and B");
+        const w128 lo = (w128)w.lo1 << 64 | w.lo0, hi = (w128)w.hi1 << 64 | w.hi0;
+        if (hi <= lo || (hi >> 96)) return pc_fail(ctx, PC_INVALID, "invalid window interval");
+        if (w.width == 0 || w.end <= w.first) return pc_fail(ctx, PC_INVALID, "invalid window v range");
+        const w128 ulo = (lo + (w128)w.first * f->A) / f->B + 1, uhi = (hi + (w128)(w.end - 1) * f->A) / f->B + 1;
+        if (uhi >> 64) return pc_fail(ctx, PC_INVALID, "u window exceeds 64 bits");
+        const uint64_t nt = (w.end - w.first + w.width - 1) / w.width;
+        if (!tiles_fit(w.first, w.end, w.width, nt)) return pc_fail(ctx, PC_INVALID, "inconsistent subtile geometry");
+        tile_base[i] = (uint32_t)ntiles;
+        ntiles += nt;
+        if (ntiles >= (UINT64_C(1) << 31)) return pc_fail(ctx, PC_INVALID, "too many subtiles");
+        focs[i] = fa;
+        lows[i] = (uint64_t)ulo;
+        highs[i] = (uint64_t)uhi;
+        pads[i] = SEG_ALIGN;
+        focs[nwin + i] = fb;
+        lows[nwin + i] = w.first;
+        highs[nwin + i] = w.end;
+        pads[nwin + i] = 1;
+        if (fam_map[w.family] == UINT32_MAX) {
+            fam_map[w.family] = (uint32_t)used.size();
+            used.push_back(f);
+        }
+    }
+    tile_base[nwin] = (uint32_t)ntiles;
+    pc_multi *m = new pc_multi(ctx);
+    m->nwin = nwin;
+    m->tile_base = tile_base;
+    int rc = winbatch_plan(ctx, m->hold, focs.data(), lows.data(), highs.data(), pads.data(), 2 * nwin,
+                           (UINT64_C(1) << 32) - 1, m->wb, nullptr);
+    if (!rc) rc = m->hold.get(&m->d_lists, std::max<uint64_t>(1, m->wb.out_len));
+    if (rc) {
+        delete m;
+        return rc;
+    }
+    const uint64_t vstart = m->wb.base[nwin];
+    Engine &E = m->E;
+    E.us = m->d_lists;
+    E.nu = vstart;
+    E.vs = m->d_lists + vstart;
+    E.nv = m->wb.out_len - vstart;
+    E.fams = used;
+    E.ntiles = ntiles;
+    E.out_cap = out_cap;
+    E.tile_seg.resize(ntiles);
+    m->sizes.resize(2 * (size_t)nwin);
+    for (uint32_t i = 0; i < nwin; ++i) {
+        const pc_window &w = windows[i];
+        const pc_filters *f = families[w.family];
+        SegDev g{};
+        g.A = f->A;
+        g.B = f->B;
+        g.lo = u128{w.lo0, w.lo1};
+        g.hi = u128{w.hi0, w.hi1};
+        g.v_first = w.first;
+        g.width = w.width;
+        g.v_end = w.end;
+        g.u_off = (uint32_t)m->wb.base[i];
+        g.nu = (uint32_t)m->wb.total[i];
+        g.v_off = (uint32_t)(m->wb.base[nwin + i] - vstart);
+        g.nv = (uint32_t)m->wb.total[nwin + i];
+        g.tile_base = tile_base[i];
+        g.ntiles = tile_base[i + 1] - tile_base[i];
+        g.fam = fam_map[w.family];
+        E.segs.push_back(g);
+        for (uint32_t t = tile_base[i]; t < tile_base[i + 1]; ++t) E.tile_seg[t] = i;
+        m->sizes[2 * i] = g.nu;
+        m->sizes[2 * i + 1] = g.nv;
+    }
+    rc = engine_prepare(E, tuning, m->hold);
+    if (!rc) rc = pc_cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "window batch set-up");
+    if (rc) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return PC_OK;
+}
+
+namespace {
+
+int multi_eager(pc_ctx *ctx, pc_multi *m, pc_stats *stats) {
+    Engine &E = m->E;
+    int launches = 0;
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
+    int rc = winbatch_count(ctx, m->wb);
+    if (!rc) rc = winbatch_emit(ctx, m->wb, m->d_lists);
+    if (rc) return rc;
+    launches += 5;
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[5], ctx->stream));
+    rc = engine_eager(E, &launches);
+    if (rc) return rc;
+    m->counts.assign(E.ntiles * E.stride, 0);
+    m->geometry.assign(2 * E.ntiles, 0);
+    m->out.assign(2 * std::max<uint64_t>(1, E.out_cap), 0);
+    rc = engine_collect(E, m->counts.data(), m->geometry.data(), m->out.data(), &m->n_out);
+    m->launches = launches;
+    if (!rc || rc == PC_OVERFLOW || rc == PC_ARITHMETIC) {
+        engine_stats(E, stats, launches, m->n_out);
+        if (stats) stats->window_ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+    }
+    return rc;
+}
+
+// Records the whole run (windows, stages 2 and 3, and the copies of the counters) into a graph.
+// The deep tier's grid and slice capacity come from the eager run that precedes the capture.
+int multi_capture(pc_ctx *ctx, pc_multi *m) {
+    Engine &E = m->E;
+    cudaStream_t st = ctx->stream;
+    const uint64_t nc = std::max<uint64_t>(1, E.ntiles * E.stride), ng = std::max<uint64_t>(1, 2 * E.ntiles);
+    if (!m->h_counts) {
+        PC_CHECK(ctx, cudaMallocHost((void **)&m->h_counts, nc * 8));
+        PC_CHECK(ctx, cudaMallocHost((void **)&m->h_geo, ng * 8));
+        PC_CHECK(ctx, cudaMallocHost((void **)&m->h_nout, 16));
+        PC_CHECK(ctx, cudaMallocHost((void **)&m->h_deep, (uint64_t)E.grid * 4));
+    }
+    int rc = engine_match(E, 2);
+    if (rc) return rc;
+    PC_CHECK(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int launches = 0;
+    rc = winbatch_count(ctx, m->wb);
+    if (!rc) rc = winbatch_emit(ctx, m->wb, m->d_lists);
+    if (!rc) rc = engine_front(E, false, true, &launches);
+    if (!rc) rc = engine_back(E, false, &launches);
+    if (!rc) rc = pc_cuda_status(ctx, cudaMemcpyAsync(m->h_nout, E.d_nout, 16, cudaMemcpyDeviceToHost, st), "capture copy");
+    if (!rc && E.ntiles) {
+        rc = pc_cuda_status(ctx, cudaMemcpyAsync(m->h_counts, E.d_counts, E.ntiles * E.stride * 8, cudaMemcpyDeviceToHost, st),
+                            "capture copy");
+        if (!rc)
+            rc = pc_cuda_status(ctx, cudaMemcpyAsync(m->h_geo, E.d_geo, 2 * E.ntiles * 8, cudaMemcpyDeviceToHost, st),
+                                "capture copy");
+    }
+    if (!rc)
+        rc = pc_cuda_status(ctx, cudaMemcpyAsync(m->h_deep, E.d_deep_count, (uint64_t)E.grid * 4, cudaMemcpyDeviceToHost, st),
+                            "capture copy");
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);       // always leave capture mode
+    if (!rc && e != cudaSuccess) rc = pc_cuda_fail(ctx, e, "end capture");
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc;
+    }
+    m->graph = g;
+    PC_CHECK(ctx, cudaGraphInstantiate(&m->exec, g, 0));
+    m->launches = launches + 5;
+    return PC_OK;
+}
+
+int multi_replay(pc_ctx *ctx, pc_multi *m, pc_stats *stats) {
+    Engine &E = m->E;
+    cudaStream_t st = ctx->stream;
+    int rc = engine_match(E, 2);                          // another object may have lowered the limit
+    if (rc) return rc;
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[0], st));
+    PC_CHECK(ctx, cudaGraphLaunch(m->exec, st));
+    PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], st));
+    PC_CHECK(ctx, cudaStreamSynchronize(st));
+    for (int b = 0; b < E.grid; ++b)
+        if (m->h_deep[b] > E.deep_cap) return pc_fail(ctx, PC_ARITHMETIC, "deep survivor count changed between runs");
+    m->counts.assign(m->h_counts, m->h_counts + E.ntiles * E.stride);
+    m->geometry.assign(m->h_geo, m->h_geo + 2 * E.ntiles);
+    const unsigned long long nout[2] = {m->h_nout[0], m->h_nout[1]};
+    m->n_out = nout[0];
+    rc = engine_check(E, nout, m->counts.data());
+    if (!rc && nout[0]) {
+        PC_CHECK(ctx, cudaMemcpyAsync(m->out.data(), E.d_out, 2 * nout[0] * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, cudaStreamSynchronize(st));
+    }
+    if (stats) {
+        stats->kernel_ms = elapsed_ms(ctx->ev[0], ctx->ev[1]);
+        stats->outputs = m->n_out;
+        stats->launches = m->launches;
+        stats->work_items = E.deep_max;
+        stats->reserved[0] = E.tn.nb;
+        stats->reserved[1] = E.tn.K;
+        stats->reserved[2] = E.tn.threads;
+        stats->reserved[3] = E.tn.nch;
+        stats->reserved[4] = 1;
+    }
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int pc_multi_run(pc_ctx *ctx, pc_multi *m, uint32_t flags, pc_stats *stats) {
+    if (!m) return pc_fail(ctx, PC_INVALID, "no window batch");
+    if (stats) memset(stats, 0, sizeof(*stats));
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = PC_OK;
+    if (!(flags & PC_RUN_GRAPH) || !m->ran) {
+        rc = multi_eager(ctx, m, stats);
+        if (!rc) m->ran = true;
+    }
+    if (!rc && (flags & PC_RUN_GRAPH)) {
+        if (!m->exec) rc = multi_capture(ctx, m);
+        if (!rc) rc = multi_replay(ctx, m, stats);
+    }
+    if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+extern "C" int pc_multi_layout(const pc_multi *m, uint32_t *tile_base, uint64_t *sizes, uint64_t *info) {
+    if (!m) return PC_INVALID;
+    const Engine &E = m->E;
+    if (tile_base) std::copy(m->tile_base.begin(), m->tile_base.end(), tile_base);
+    if (sizes) std::copy(m->sizes.begin(), m->sizes.end(), sizes);
+    if (info) {
+        info[0] = E.ntiles;
+        info[1] = E.stride;
+        info[2] = E.nu;
+        info[3] = E.nv;
+        info[4] = E.deep_cap;
+        info[5] = E.tn.nb;
+        info[6] = E.tn.K;
+        info[7] = E.tn.threads;
+    }
+    return PC_OK;
+}
+
+extern "C" int pc_multi_results(pc_ctx *ctx, const pc_multi *m, uint64_t *counts, uint64_t *geometry, uint64_t *out,
+                                uint64_t out_cap, uint64_t *n_out) {
+    if (!m || !m->ran) return pc_fail(ctx, PC_INVALID, "window batch has not run");
+    if (counts) std::copy(m->counts.begin(), m->counts.end(), counts);
+    if (geometry) std::copy(m->geometry.begin(), m->geometry.end(), geometry);
+    *n_out = m->n_out;
+    if (out) std::copy(m->out.begin(), m->out.begin() + 2 * std::min(m->n_out, out_cap), out);
+    return PC_OK;
+}
+
+extern "C" int pc_multi_free(pc_ctx *ctx, pc_multi *m) {
+    if (!m) return PC_OK;
+    cudaStreamSynchronize(ctx->stream);
+    delete m;
     return PC_OK;
 }
 

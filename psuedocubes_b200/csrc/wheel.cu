@@ -109,14 +109,23 @@ struct WindowPlan {
     uint64_t units_first, units_mid, units_last, units;
 };
 
-struct WindowArgs {
+// Device view of one focus: the sorted wheel and the bitset rows of its T rings.
+struct FocusDev {
+    const uint64_t *W1;
+    const uint32_t *rows;
     uint64_t M1, count1, words1;
-    uint32_t nT;
+    uint32_t nT, pad;
     uint32_t tq[PC_MAX_WHEEL_T];
     uint32_t t_m1mod[PC_MAX_WHEEL_T];
     uint32_t t_row0[PC_MAX_WHEEL_T];
     ModQ tmq[PC_MAX_WHEEL_T];
+};
+
+// One window of a batch: its plan, its first unit in the batch-wide unit numbering and its focus.
+struct WinDesc {
     WindowPlan plan;
+    uint64_t unit_base;
+    uint32_t focus, pad;
 };
 
 __device__ __forceinline__ void unit_of(const WindowPlan &p, uint64_t words1, uint64_t u, uint64_t &K,
@@ -144,26 +153,37 @@ __device__ __forceinline__ void unit_of(const WindowPlan &p, uint64_t words1, ui
 }
 
 // One warp per window unit of WIN_WORDS = 32 wheel words, one word per lane, so every row load
-// of the warp is one coalesced 128-byte request.  Count pass: per-unit totals.  Emit pass: the
-// lane's exclusive prefix inside the warp plus the unit's offset gives ascending output slots.
-__global__ void k_window(const WindowArgs a, const uint64_t *__restrict__ W1, const uint32_t *__restrict__ rows,
-                         uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
-                         uint64_t *__restrict__ out) {
+// of the warp is one coalesced 128-byte request.  The warp finds its window by a binary search
+// over the windows' first units.  Count pass: per-unit totals.  Emit pass: the lane's exclusive
+// prefix inside the warp, plus the unit's offset inside its window, plus the window's base gives
+// ascending output slots.
+__global__ void k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, const FocusDev *__restrict__ foci,
+                          uint64_t units, uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
+                          const uint64_t *__restrict__ bases, uint64_t *__restrict__ out) {
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t u = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    if (u >= a.plan.units) return;                      // warp-uniform
+    const uint64_t gu = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    if (gu >= units) return;                            // warp-uniform
+    uint32_t lo = 0, hi = ndesc;                        // last window with unit_base <= gu
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (desc[mid].unit_base <= gu) lo = mid;
+        else hi = mid;
+    }
+    const WindowPlan &p = desc[lo].plan;
+    const uint64_t ubase = desc[lo].unit_base;
+    const FocusDev &f = foci[desc[lo].focus];
     uint64_t K, wa, wb;
-    unit_of(a.plan, a.words1, u, K, wa, wb);
+    unit_of(p, f.words1, gu - ubase, K, wa, wb);
     const uint64_t w = wa + lane;
     uint32_t bits = 0;
     if (w < wb) {
         bits = 0xffffffffu;
-        for (uint32_t t = 0; t < a.nT; ++t) {
-            const uint32_t s = fastmod32(mod64(K, a.tmq[t]) * a.t_m1mod[t], a.tmq[t].c, a.tq[t]);   // < q^2 < 2^32
-            bits &= __ldg(rows + (uint64_t)(a.t_row0[t] + s) * a.words1 + w);
+        for (uint32_t t = 0; t < f.nT; ++t) {
+            const uint32_t s = fastmod32(mod64(K, f.tmq[t]) * f.t_m1mod[t], f.tmq[t].c, f.tq[t]);   // < q^2 < 2^32
+            bits &= __ldg(f.rows + (uint64_t)(f.t_row0[t] + s) * f.words1 + w);
         }
-        const uint64_t jmin = K == a.plan.K0 ? a.plan.j_lo : 0;
-        const uint64_t jmax = K == a.plan.K1 ? a.plan.j_hi : a.count1;
+        const uint64_t jmin = K == p.K0 ? p.j_lo : 0;
+        const uint64_t jmax = K == p.K1 ? p.j_hi : f.count1;
         const uint64_t j0 = w * 32;
         if (j0 < jmin) bits &= ~low_bits((uint32_t)(jmin - j0 < 32 ? jmin - j0 : 32));
         if (j0 + 32 > jmax) bits &= jmax > j0 ? low_bits((uint32_t)(jmax - j0)) : 0u;
@@ -171,7 +191,7 @@ __global__ void k_window(const WindowArgs a, const uint64_t *__restrict__ W1, co
     const uint32_t n = __popc(bits);
     if (!offsets) {
         const uint32_t total = __reduce_add_sync(0xffffffffu, n);
-        if (lane == 0) counts[u] = total;
+        if (lane == 0) counts[gu] = total;
         return;
     }
     uint32_t incl = n;
@@ -180,13 +200,22 @@ __global__ void k_window(const WindowArgs a, const uint64_t *__restrict__ W1, co
         const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
         if (lane >= (uint32_t)d) incl += y;
     }
-    uint64_t pos = offsets[u] + incl - n;
-    const uint64_t base = K * a.M1, j0 = w * 32;
+    uint64_t pos = bases[lo] + (offsets[gu] - offsets[ubase]) + incl - n;
+    const uint64_t base = K * f.M1, j0 = w * 32;
     while (bits) {
         const uint32_t b = __ffs(bits) - 1;
         bits &= bits - 1;
-        out[pos++] = base + __ldg(W1 + j0 + b);
+        out[pos++] = base + __ldg(f.W1 + j0 + b);
     }
+}
+
+// Per window: its value count (offsets hold units + 1 entries, the total last).
+__global__ void k_window_totals(const WinDesc *__restrict__ desc, uint32_t ndesc, const uint64_t *__restrict__ offsets,
+                                uint64_t *__restrict__ totals) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= ndesc) return;
+    const uint64_t b = desc[w].unit_base;
+    totals[w] = offsets[b + desc[w].plan.units] - offsets[b];
 }
 
 // 128-bit product of 64-bit counts, host side.
@@ -388,6 +417,8 @@ extern "C" int pc_focus_create(pc_ctx *ctx, uint64_t M, uint32_t nrings, const u
     return PC_OK;
 }
 
+uint64_t pc_focus_modulus(const pc_focus *f) { return f->M; }
+
 extern "C" int pc_focus_free(pc_ctx *ctx, pc_focus *f) {
     if (!f) return PC_OK;
     pc_release(ctx, f->W1, f->W1_bytes);
@@ -408,28 +439,14 @@ extern "C" int pc_focus_info(const pc_focus *f, uint64_t *info) {
     return PC_OK;
 }
 
-// Plan and run one window; out is allocated by the call (out_bytes returned for release).
-// total_host receives the count.  Exported to the batch/lease code through this declaration.
-int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, uint64_t cap,
-                   uint64_t **out, uint64_t *out_bytes, uint64_t *total_host, int *launches) {
-    *out = nullptr;
-    *out_bytes = 0;
-    *total_host = 0;
+namespace {
+
+// Host plan of the window [low, high) of focus f: period and wheel-index range, units per part.
+int plan_window(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, WindowPlan &p) {
+    p = WindowPlan{};
     if (high < low) return pc_fail(ctx, PC_INVALID, "invalid bounded focus window");
     if (high == low) return PC_OK;
     if ((high - 1) / f->M - low / f->M + 1 > 4096) return pc_fail(ctx, PC_OVERFLOW, "focus window exceeds bounded period count");
-    WindowArgs a{};
-    a.M1 = f->M1;
-    a.count1 = f->count1;
-    a.words1 = f->words1;
-    a.nT = f->nT;
-    for (uint32_t t = 0; t < f->nT; ++t) {
-        a.tq[t] = f->tq[t];
-        a.t_m1mod[t] = f->t_m1mod[t];
-        a.t_row0[t] = f->t_row0[t];
-        a.tmq[t] = make_modq(f->tq[t]);
-    }
-    WindowPlan &p = a.plan;
     p.K0 = low / f->M1;
     p.K1 = (high - 1) / f->M1;
     const std::vector<uint64_t> &W = f->W1_host;
@@ -450,32 +467,130 @@ int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, 
     p.units_last = p.K1 > p.K0 ? (p.wb1 - p.wa1 + WIN_WORDS - 1) / WIN_WORDS : 0;
     uint64_t mid_periods = p.K1 > p.K0 + 1 ? p.K1 - p.K0 - 1 : 0;
     p.units = p.units_first + mid_periods * p.units_mid + p.units_last;
-    if (p.units == 0) return PC_OK;
     if (p.units >= (UINT64_C(1) << 31)) return pc_fail(ctx, PC_OVERFLOW, "focus window too long");
-    Scratch s(ctx);
-    uint64_t *d_cnt, *d_off, *d_total;
-    int rc = s.get(&d_cnt, p.units);
-    if (!rc) rc = s.get(&d_off, p.units);
-    if (!rc) rc = s.get(&d_total, 1);
+    return PC_OK;
+}
+
+FocusDev focus_dev(const pc_focus *f) {
+    FocusDev d{};
+    d.W1 = f->W1;
+    d.rows = f->rows;
+    d.M1 = f->M1;
+    d.count1 = f->count1;
+    d.words1 = f->words1;
+    d.nT = f->nT;
+    for (uint32_t t = 0; t < f->nT; ++t) {
+        d.tq[t] = f->tq[t];
+        d.t_m1mod[t] = f->t_m1mod[t];
+        d.t_row0[t] = f->t_row0[t];
+        d.tmq[t] = make_modq(f->tq[t]);
+    }
+    return d;
+}
+
+}  // namespace
+
+int winbatch_count(pc_ctx *ctx, const WinBatch &wb) {
+    if (wb.units) {
+        const unsigned grid = (unsigned)((wb.units * 32 + WT - 1) / WT);
+        k_windows<<<grid, WT, 0, ctx->stream>>>((const WinDesc *)wb.d_desc, wb.n, (const FocusDev *)wb.d_foci, wb.units,
+                                                wb.d_cnt, nullptr, nullptr, nullptr);
+        PC_LAUNCHED(ctx, "window count");
+    }
+    return pc_exclusive_scan_ws(ctx, wb.d_cnt, wb.d_off, wb.units, wb.d_off + wb.units, wb.d_ws);
+}
+
+int winbatch_emit(pc_ctx *ctx, const WinBatch &wb, uint64_t *out) {
+    if (!wb.out_len) return PC_OK;
+    PC_CHECK(ctx, cudaMemsetAsync(out, 0, wb.out_len * 8, ctx->stream));   // padding slots read as 0
+    if (wb.units) {
+        const unsigned grid = (unsigned)((wb.units * 32 + WT - 1) / WT);
+        k_windows<<<grid, WT, 0, ctx->stream>>>((const WinDesc *)wb.d_desc, wb.n, (const FocusDev *)wb.d_foci, wb.units,
+                                                nullptr, wb.d_off, wb.d_base, out);
+        PC_LAUNCHED(ctx, "window emit");
+    }
+    return PC_OK;
+}
+
+int winbatch_plan(pc_ctx *ctx, Scratch &hold, const pc_focus *const *focus, const uint64_t *low, const uint64_t *high,
+                  const uint64_t *pad, uint32_t n, uint64_t cap, WinBatch &wb, int *launches) {
+    wb = WinBatch{};
+    wb.n = n;
+    if (!n) return PC_OK;
+    std::vector<WinDesc> desc(n);
+    std::vector<FocusDev> foci;
+    std::vector<const pc_focus *> seen;
+    for (uint32_t i = 0; i < n; ++i) {
+        int rc = plan_window(ctx, focus[i], low[i], high[i], desc[i].plan);
+        if (rc) return rc;
+        desc[i].unit_base = wb.units;
+        wb.units += desc[i].plan.units;
+        uint32_t k = 0;
+        while (k < seen.size() && seen[k] != focus[i]) ++k;
+        if (k == seen.size()) {
+            seen.push_back(focus[i]);
+            foci.push_back(focus_dev(focus[i]));
+        }
+        desc[i].focus = k;
+    }
+    if (wb.units >= (UINT64_C(1) << 34)) return pc_fail(ctx, PC_OVERFLOW, "focus windows too long");
+    WinDesc *d_desc;
+    FocusDev *d_foci;
+    int rc = hold.get(&d_desc, n);
+    if (!rc) rc = hold.get(&d_foci, foci.size());
+    if (!rc) rc = hold.get(&wb.d_cnt, std::max<uint64_t>(1, wb.units));
+    if (!rc) rc = hold.get(&wb.d_off, wb.units + 1);
+    if (!rc) rc = hold.get(&wb.d_ws, pc_scan_workspace(wb.units));
+    if (!rc) rc = hold.get(&wb.d_tot, n);
+    if (!rc) rc = hold.get(&wb.d_base, n);
     if (rc) return rc;
-    unsigned grid = (unsigned)((p.units * 32 + WT - 1) / WT);
-    k_window<<<grid, WT, 0, ctx->stream>>>(a, f->W1, f->rows, d_cnt, nullptr, nullptr);
-    PC_LAUNCHED(ctx, "window count");
-    rc = pc_exclusive_scan_u64(ctx, d_cnt, d_off, p.units, d_total);
+    wb.d_desc = d_desc;
+    wb.d_foci = d_foci;
+    PC_CHECK(ctx, cudaMemcpyAsync(d_desc, desc.data(), n * sizeof(WinDesc), cudaMemcpyHostToDevice, ctx->stream));
+    PC_CHECK(ctx, cudaMemcpyAsync(d_foci, foci.data(), foci.size() * sizeof(FocusDev), cudaMemcpyHostToDevice, ctx->stream));
+    rc = winbatch_count(ctx, wb);
     if (rc) return rc;
-    uint64_t total = 0;
-    PC_CHECK(ctx, cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    k_window_totals<<<(n + 255) / 256, 256, 0, ctx->stream>>>(d_desc, n, wb.d_off, wb.d_tot);
+    PC_LAUNCHED(ctx, "window totals");
+    wb.total.assign(n, 0);
+    PC_CHECK(ctx, cudaMemcpyAsync(wb.total.data(), wb.d_tot, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
     PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
-    *total_host = total;
-    if (total > cap) return pc_fail(ctx, PC_OVERFLOW, "focus buffer overflow; tile invalid");
-    uint64_t bytes = std::max<uint64_t>(16, total * 8);
+    wb.base.assign(n, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (wb.total[i] > cap) return pc_fail(ctx, PC_OVERFLOW, "focus buffer overflow; tile invalid");
+        const uint64_t pd = pad && pad[i] ? pad[i] : 1;
+        wb.base[i] = (wb.out_len + pd - 1) / pd * pd;
+        wb.out_len = wb.base[i] + wb.total[i];
+    }
+    PC_CHECK(ctx, cudaMemcpyAsync(wb.d_base, wb.base.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));   // the host vectors above go out of scope
+    if (launches) *launches += 4;
+    return PC_OK;
+}
+
+// Plan and run one window; out is allocated by the call (out_bytes returned for release).
+// total_host receives the count.
+int pc_window_into(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, uint64_t cap,
+                   uint64_t **out, uint64_t *out_bytes, uint64_t *total_host, int *launches) {
+    *out = nullptr;
+    *out_bytes = 0;
+    *total_host = 0;
+    if (high < low) return pc_fail(ctx, PC_INVALID, "invalid bounded focus window");
+    if (high == low) return PC_OK;
+    Scratch s(ctx);
+    WinBatch wb;
+    int rc = winbatch_plan(ctx, s, &f, &low, &high, nullptr, 1, UINT64_MAX, wb, launches);
+    if (rc) return rc;
+    *total_host = wb.total[0];
+    if (wb.total[0] > cap) return pc_fail(ctx, PC_OVERFLOW, "focus buffer overflow; tile invalid");
+    if (!wb.out_len) return PC_OK;
+    const uint64_t bytes = std::max<uint64_t>(16, wb.out_len * 8);
     rc = pc_alloc(ctx, (void **)out, bytes);
     if (rc) return rc;
     *out_bytes = bytes;
-    k_window<<<grid, WT, 0, ctx->stream>>>(a, f->W1, f->rows, nullptr, d_off, *out);
-    PC_LAUNCHED(ctx, "window emit");
-    if (launches) *launches += 2 + 3;
-    return PC_OK;
+    rc = winbatch_emit(ctx, wb, *out);
+    if (launches) *launches += 1;
+    return rc;
 }
 
 extern "C" int pc_focus_window(pc_ctx *ctx, const pc_focus *f, uint64_t low, uint64_t high, uint64_t cap,
