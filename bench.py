@@ -260,6 +260,111 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+WINDOWS_METRIC = 'focused candidate positions/s (512 uneven windows, p in [499, 619], CUDA-graph replay)'
+
+
+def run_windows(args) -> None:
+    """Batched uneven windows: 512 seeded windows (span floor(10^U(6,10)) v, first uniform in
+    [0, B - span), p uniform over the primes in [499, 619] with p = 1 mod 3) in one launch
+    sequence replayed as a CUDA graph; beside it the plain per-window tile loop of the same build
+    on a sample of the windows, checked window by window."""
+    from psuedocubes_b200.batched import Autotuner, BatchedEngine, DEFAULT_SETTINGS, seeded_windows, workload_digest
+    from psuedocubes_b200.gpu import Matcher, Runtime
+    from psuedocubes_b200.run_production import compute_batch
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    runtime = Runtime(time.monotonic() + 7200, 16 * 1024**3, 0.5, device=local)
+    engine = BatchedEngine(runtime)
+    windows = seeded_windows(512, 619003 + rank)
+    tuner = Autotuner(engine)
+    settings = dict(DEFAULT_SETTINGS)
+    tuned = 'defaults'
+    if args.tune:
+        settings, tuned = tuner.tune(windows, reuse=False).settings, 'tuned in this run'
+    elif tuner.load(windows):
+        settings, tuned = tuner.load(windows), 'persisted tuning'
+    tuning = {k: v for k, v in settings.items() if k != 'width'}
+    batch = engine.plan(windows, settings['width'], tuning, output_cap=1 << 16)
+    eager = batch.run()
+    for _ in range(max(1, args.warmup)):
+        batch.run(graph=True)
+    positions = batch.positions()
+    lib, ctx = runtime.lib, runtime.ctx
+    barrier(dist)
+    graph_ms = []
+    with ClockSampler(local) as clocks:
+        runtime.call(lib.pc_mark(ctx, 0))
+        for _ in range(args.steps):
+            graph_ms.append(batch.run(graph=True)['kernel_ms'])
+        runtime.call(lib.pc_mark(ctx, 1))
+        elapsed = ctypes.c_double()
+        runtime.call(lib.pc_elapsed(ctx, 0, 1, ctypes.byref(elapsed)))
+    seconds = max_over_ranks(dist, elapsed.value / 1000, local)
+    counts, geometry, records = batch.raw()
+    launches = int(batch.last_stats.get('launches', 0))
+    layout = dict(batch.layout)
+    batch.close()
+    # end to end through the public API: plan (descriptors to the device), eager run, results with
+    # host verification of every window
+    e2e_times = []
+    rows = None
+    for _ in range(max(1, args.e2e_steps)):
+        t0 = time.perf_counter()
+        b = engine.plan(windows, settings['width'], tuning, output_cap=1 << 16)
+        b.run()
+        rows = b.results()
+        b.close()
+        e2e_times.append(time.perf_counter() - t0)
+    # the plain per-window tile loop (Matcher.tile over 1e8-v tiles) on a sample, checked per window
+    sample = windows[:args.plain_windows]
+    mismatches, plain_positions = 0, 0
+    t0 = time.perf_counter()
+    for w, row in zip(sample, rows):
+        c = w.config()
+        af, bf = c.focuses()
+        want = compute_batch(Matcher(runtime, c), engine.focus(af), engine.focus(bf), w.first, w.end, 100_000_000)
+        plain_positions += want['valid_focused_candidates']
+        same = all(row[k] == want[k] for k in ('valid_focused_candidates', 'group_survivors', 'local_survivors',
+                                                'genuine_cubes', 'filter_groups'))
+        same = same and sorted(map(int, row['all_values'])) == sorted(map(int, want['all_values']))
+        mismatches += 0 if same else 1
+    plain_seconds = time.perf_counter() - t0
+    if rank == 0:
+        clock = clocks.summary()
+        sm_mhz = clock['sm_max_mhz'] or 1965.0
+        peak = runtime.sm_count * 4 * 32 * sm_mhz * 1e6 / 1e12
+        mean_graph_ms = sum(graph_ms) / len(graph_ms)
+        achieved = OPS_PER_POSITION * positions / (mean_graph_ms / 1000) / 1e12
+        d2h = counts.nbytes + geometry.nbytes + records.nbytes + 16
+        h2d = 64 * len(windows)
+        line = dict(metric=WINDOWS_METRIC, value=positions * world * args.steps / seconds, unit=UNIT, n_gpus=world,
+                    steps=args.steps, warmup=args.warmup, ms_per_step=1000 * seconds / args.steps,
+                    higher_is_better=True, scaling='weak', vs_baseline=None, dtype='u64', data='synthetic',
+                    config=dict(workload='512 windows, span floor(10^U(6,10)) v, first U[0, B619 - span), '
+                                         'p U{499..619, p = 1 mod 3}, Config(p, 10^27, 3*10^27, A619, B619)',
+                                seed=619003, windows_sha256=workload_digest(windows),
+                                span_total=sum(w.end - w.first for w in windows), positions=positions,
+                                settings=settings, settings_source=tuned, layout=layout,
+                                l2='inputs larger than L2 (wheel tables 208 MB; lists and per-v records of all windows)'),
+                    roofline=dict(bound='int_alu', achieved=achieved, peak=peak, unit='Tlaneop/s', frac=achieved / peak,
+                                  traffic=DRAM_BYTES_PER_POSITION * positions,
+                                  traffic_unit='bytes per replay (lease ncu capture, scaled by positions)',
+                                  kernel='whole graph (windows, bounds, k_match, k_deep): a lower bound for k_match',
+                                  ops_per_position=OPS_PER_POSITION),
+                    e2e=dict(value=positions * world / statistics.median(e2e_times), unit=UNIT, h2d_bytes_per_step=h2d,
+                             d2h_bytes_per_step=int(d2h), api='BatchedEngine.plan + WindowBatch.run + results'),
+                    eager=dict(ms=eager['total_ms'], kernel_ms=eager['kernel_ms'], window_ms=eager['window_ms']),
+                    plain_path=dict(value=plain_positions / plain_seconds, unit=UNIT, windows=len(sample),
+                                    seconds=plain_seconds, mismatches=mismatches,
+                                    api='run_production.compute_batch(Matcher) per window, 1e8-v tiles'),
+                    gpu_launches=launches, clocks=clock)
+        print(json.dumps(line), flush=True)
+    del batch, engine
+    runtime.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument('--gpus', type=int, default=1)
@@ -273,9 +378,16 @@ def main() -> None:
     parser.add_argument('--bitset-filters', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--block-words', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--threads', type=int, default=0, help='tuning override (0 = library default)')
+    parser.add_argument('--workload', choices=('lease', 'windows'), default='lease',
+                        help='lease: the p=619 production lease (headline); windows: 512 uneven windows')
+    parser.add_argument('--tune', action='store_true', help='windows: run the autotuner first')
+    parser.add_argument('--plain-windows', type=int, default=64,
+                        help='windows: how many windows the plain per-window loop is timed and checked on')
     args = parser.parse_args()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.workload == 'windows':
+        run_windows(args)
     else:
         run_ours(args)
 

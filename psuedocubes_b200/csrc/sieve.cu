@@ -506,10 +506,11 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         }
         for (uint32_t k = threadIdx.x; k < a.tmax * cstride; k += blockDim.x) cnt_s[k] = 0;
         __syncthreads();
-        const uint64_t sv_first = S.v_first, swidth = S.width, stn = S.ntiles, stb = S.tile_base;
-        const uint64_t seg_tiles_end = stb + stn;
+        // subtile geometry of the segment stays in shared memory (S): it is read only when a lane's
+        // subtile changes and when a queued survivor needs its subtile recomputed
+        const uint64_t seg_tiles_end = (uint64_t)S.tile_base + S.ntiles;
         const bool c2_live = F.c2_live != 0;
-        const uint64_t tile_base = stb + local_tile(a.rec[va].v, sv_first, swidth, stn);
+        const uint64_t tile_base = S.tile_base + local_tile(a.rec[va].v, S.v_first, S.width, S.ntiles);
 
         uint32_t c[3] = {0, 0, 0};
         uint64_t ctile = UINT64_MAX, t_lo = 1, t_hi = 0;  // this lane's subtile and its v range
@@ -548,7 +549,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             qhead += n;
             if (!mine) return;
             const uint32_t uidx = meta & 0xfff, slot = meta >> 12;
-            const uint64_t tile = slot == SLOT_FAR ? stb + local_tile(v, sv_first, swidth, stn) : tile_base + slot;
+            const uint64_t tile = slot == SLOT_FAR ? S.tile_base + local_tile(v, S.v_first, S.width, S.ntiles) : tile_base + slot;
             if (tile >= seg_tiles_end) return;            // v outside the subtile geometry (reported by k_vprep)
             for (uint32_t t = 0; t < nch; ++t) {
                 const uint32_t vr = fastmod32(mod64(v, F.cmq[t]) * F.caq[t], F.cmq[t].c, F.cq[t]);
@@ -587,9 +588,10 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             if (__any_sync(0xffffffffu, moved)) {
                 flush();
                 if (moved) {
-                    const uint64_t lt = local_tile(rec.v, sv_first, swidth, stn);
-                    ctile = lt < stn ? stb + lt : UINT64_MAX;
-                    t_lo = sv_first + lt * swidth;
+                    const uint64_t stn = S.ntiles, swidth = S.width;
+                    const uint64_t lt = local_tile(rec.v, S.v_first, swidth, stn);
+                    ctile = lt < stn ? S.tile_base + lt : UINT64_MAX;
+                    t_lo = S.v_first + lt * swidth;
                     t_hi = lt < stn ? t_lo + swidth : t_lo;
                 }
             }
