@@ -16,7 +16,7 @@ from typing import Any
 import numpy as np
 
 from . import _native as N
-from .accounting import digest
+from .accounting import EMPTY_DIGEST, digest, scope_list
 from .focus import Config, Tile
 from .gpu import MASK, DeviceArray, Filters, GPUFocus, Matcher, Runtime, launch_plan
 from .predicate import is_perfect_cube, local3
@@ -123,18 +123,23 @@ def batch_result(config: Config, ranges: list[tuple[int, int, int, int]], pops: 
         raise ArithmeticError('unsigned underflow')
     if np.any(pops[:, ng + 1] > output_cap):
         raise OverflowError('fused tile output overflow; no truncated coverage')
+    emitted = pops[:, ng + 1].tolist()
     all_values: list[int] = []
-    scopes = []
+    digests = []
     for row, (first, end, _, _) in enumerate(ranges):
         values = per_tile[row]
-        if len(values) != int(pops[row, ng + 1]):
+        if len(values) != emitted[row]:
             raise ArithmeticError('device output count disagrees with its records')
-        if any(not first <= config.canonical(n)[1] < end for n in values):
-            raise ArithmeticError('output assigned to wrong subtile')
-        all_values.extend(values)
-        scopes.append(dict(first=str(first), end=str(end), valid_focused_candidates=int(pops[row, 0]),
-                           group_survivors=[int(n) for n in pops[row, 1:ng + 1]], local_survivors=len(values),
-                           output_sha256=digest([str(n) for n in values])))
+        if values:
+            if any(not first <= config.canonical(n)[1] < end for n in values):
+                raise ArithmeticError('output assigned to wrong subtile')
+            all_values.extend(values)
+            digests.append(digest([str(n) for n in values]))
+        else:
+            digests.append(EMPTY_DIGEST)
+    scopes = scope_list([r[0] for r in ranges], [r[1] for r in ranges], pops[:, 0].tolist(),
+                        pops[:, 1:ng + 1].tolist(), emitted, digests,
+                        below_2_53=int(pops[:, :ng + 2].max(initial=0)) < 1 << 53)
     hits = verify_values(config, all_values)
     groups = [int(n) for n in pops[:, 1:ng + 1].sum(axis=0)] if len(ranges) else [0] * ng
     return dict(status='PASS', host_verified=True, focus_u=sum(u for u, _ in geometry),

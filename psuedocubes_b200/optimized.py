@@ -12,8 +12,9 @@ import hashlib
 import time
 from typing import Any, Callable
 
-from .accounting import digest, encoded
-from .batch_experiment import MaskedMatcher, batch_result, prepare, tile_ranges
+from .accounting import digest, encoded_scopes
+from .batch_experiment import MaskedMatcher, batch_result, prepare
+from .focus import Tile
 from .gpu import GPUFocus
 from .multi import validate_result
 
@@ -67,7 +68,7 @@ class Accumulator:
             self.groups[i] += int(count)
         self.values.extend(row['all_values'])
         self.hits.extend(row['cpu_confirmed_hits'])
-        self.transcript.update(encoded(row['subtile_scopes']))
+        self.transcript.update(encoded_scopes(row['subtile_scopes']))
         self.batches += 1
         self.subtiles += len(actual)
         self.cursor = end
@@ -92,6 +93,7 @@ class Accumulator:
 def lease_batches(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, first: int, end: int) -> list[tuple[int, int, dict[str, Any]]]:
     """Every batch result of [first, end) from one fused lease call, in batch order."""
     width = PROFILE['tile_width']
+    Tile(first, end).validate(matcher.config)
     raw = matcher.run_lease(af, bf, first, end, width)
     stats = raw['stats']
     nbatches = (end - first + BATCH_WIDTH - 1) // BATCH_WIDTH
@@ -99,7 +101,9 @@ def lease_batches(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, first: int
     for k in range(nbatches):
         start = first + k * BATCH_WIDTH
         stop = min(start + BATCH_WIDTH, end)
-        ranges = tile_ranges(matcher.config, start, stop, width)
+        # subtile bounds only: batch_result reads (first, end) and the lease call already checked
+        # the geometry on the device
+        ranges = [(v, min(v + width, stop), 0, 0) for v in range(start, stop, width)]
         t0 = k * PROFILE['tiles_per_compute_batch']
         rows = slice(t0, t0 + len(ranges))
         geometry = [(int(a), int(b)) for a, b in raw['geometry'][rows]]

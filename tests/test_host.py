@@ -143,3 +143,27 @@ def test_status_codes_map_to_reference_exceptions():
         with pytest.raises(exc):
             N.raise_for(code, None, 'x')
     N.raise_for(N.PC_OK)
+
+
+def test_scope_encoding_matches_canonical_json():
+    """The transcript bytes built from counter arrays equal encoded() of the scope dicts, including
+    counters at and above 2^53 (which the canonical form writes as strings)."""
+    import random
+    from psuedocubes_b200.accounting import EMPTY_DIGEST, digest, encoded, encoded_scopes, scope_list
+    assert EMPTY_DIGEST == digest([]) == '37517e5f3dc66819f61f5a7bb8ace1921282415f10551d2defa5c3eb0985b570'
+    rng = random.Random(619)
+    for trial in range(60):
+        n, ng = rng.randint(0, 70), rng.randint(0, 24)
+        top = (1 << 53) + 5 if trial % 4 == 0 else 10**9
+        firsts = sorted(rng.randrange(0, 10**18) for _ in range(n))
+        ends = [f + rng.randrange(1, 10**8) for f in firsts]
+        valid = [rng.randrange(0, top) for _ in range(n)]
+        groups = [[rng.randrange(0, top) for _ in range(ng)] for _ in range(n)]
+        local = [rng.randrange(0, 9000) for _ in range(n)]
+        digests = [rng.choice([EMPTY_DIGEST, digest([str(rng.randrange(10**27))])]) for _ in range(n)]
+        safe = top < 1 << 53
+        scopes = scope_list(firsts, ends, valid, groups, local, digests, below_2_53=safe and trial % 2 == 1)
+        assert encoded_scopes(scopes) == encoded(list(scopes))
+        assert list(scopes) == [dict(first=str(f), end=str(e), valid_focused_candidates=v, group_survivors=g,
+                                     local_survivors=k, output_sha256=d)
+                                for f, e, v, g, k, d in zip(firsts, ends, valid, groups, local, digests)]
