@@ -365,6 +365,64 @@ def run_windows(args) -> None:
         dist.destroy_process_group()
 
 
+SERVED_METRIC = 'served focused positions/s and p50/p99 latency (Poisson 20 req/s range certification)'
+
+
+def run_served(args) -> None:
+    """Served range certification: Poisson arrivals at 20 requests/s of (p, x_lo, x_hi), p uniform
+    over the accepted primes in [499, 619], x_lo = 10^U(20, log10 3e27), span = 10^U(15, 22),
+    admitted by device memory under an 8 GiB cap, continuous batching; beside it the sequential
+    plain per-request loop on the same arrival stream, under a time limit."""
+    from psuedocubes_b200.gpu import Runtime
+    from psuedocubes_b200.served import ServedLoop, latency_summary, plain_loop, poisson_requests
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    runtime = Runtime(time.monotonic() + 7200, 8 * 1024**3, 0.5, device=local)
+    requests = poisson_requests(args.requests, rate=20.0, seed=619003 + rank)
+    warm = [r for r in poisson_requests(40, rate=20.0, seed=7) if r.hi - r.lo <= 10**17][:3]
+    ServedLoop(runtime).run(warm, realtime=False)
+    barrier(dist)
+    loop = ServedLoop(runtime)
+    with ClockSampler(local) as clocks:
+        served = loop.run(requests, realtime=True, time_limit=args.served_limit)
+    served_summary = latency_summary(served, requests)
+    print(json.dumps(dict(served=served_summary, seconds=served['seconds'])), file=sys.stderr, flush=True)
+    plain = plain_loop(runtime, requests, time_limit=args.plain_limit)
+    plain_summary = latency_summary(plain, requests)
+    mismatches = compared = 0
+    for rid, want in plain['results'].items():
+        got = served['results'].get(rid)
+        if got is None:
+            continue
+        compared += 1
+        keys = ('valid_focused_candidates', 'group_survivors', 'local_survivors', 'genuine_cubes', 'output_sha256')
+        mismatches += any(got[k] != want[k] for k in keys)
+    kernel_ms = sum(s['kernel_ms'] for s in loop.steps)
+    breakdown = {k: sum(s[k] for s in loop.steps) for k in ('window_ms', 'bounds_ms', 'kernel_ms', 'total_ms',
+                                                             'u_entries', 'v_entries', 'positions', 'windows')}
+    if rank == 0:
+        line = dict(metric=SERVED_METRIC, value=served_summary['positions_per_second'], unit=UNIT, n_gpus=world,
+                    steps=len(loop.steps), warmup=len(warm), ms_per_step=1000 * served['seconds'] / max(1, len(loop.steps)),
+                    higher_is_better=True, scaling='weak', vs_baseline=None, dtype='u64', data='synthetic',
+                    config=dict(workload='Poisson 20 req/s; p U{499..619, p = 1 mod 3}; x_lo = 10^U(20, log10 3e27); '
+                                         'span = 10^U(15, 22); per-request focus split; 8 GiB admission cap',
+                                requests=len(requests), seed=619003, arrival_span_s=requests[-1].arrival,
+                                served_time_limit_s=args.served_limit, plain_time_limit_s=args.plain_limit),
+                    served=dict(served_summary, seconds=served['seconds'], positions=served['positions'],
+                                device_ms=kernel_ms, device_busy=kernel_ms / 1000 / served['seconds'],
+                                breakdown=breakdown),
+                    plain_path=dict(plain_summary, seconds=plain['seconds'], positions=plain['positions'],
+                                    api='sequential plain per-request loop (Matcher.tile over the same windows)'),
+                    compared_requests=compared, mismatches=mismatches,
+                    e2e=dict(value=served_summary['positions_per_second'], unit=UNIT, h2d_bytes_per_step=None,
+                             d2h_bytes_per_step=None, api='ServedLoop.run (requests in, verified results out)'),
+                    gpu_launches=None, clocks=clocks.summary())
+        print(json.dumps(line), flush=True)
+    runtime.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument('--gpus', type=int, default=1)
@@ -378,8 +436,12 @@ def main() -> None:
     parser.add_argument('--bitset-filters', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--block-words', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--threads', type=int, default=0, help='tuning override (0 = library default)')
-    parser.add_argument('--workload', choices=('lease', 'windows'), default='lease',
-                        help='lease: the p=619 production lease (headline); windows: 512 uneven windows')
+    parser.add_argument('--workload', choices=('lease', 'windows', 'served'), default='lease',
+                        help='lease: the p=619 production lease (headline); windows: 512 uneven windows; '
+                             'served: Poisson range-certification requests')
+    parser.add_argument('--requests', type=int, default=100, help='served: requests in the arrival stream')
+    parser.add_argument('--served-limit', type=float, default=240.0, help='served: seconds before the loop stops')
+    parser.add_argument('--plain-limit', type=float, default=60.0, help='served: seconds for the plain loop')
     parser.add_argument('--tune', action='store_true', help='windows: run the autotuner first')
     parser.add_argument('--plain-windows', type=int, default=64,
                         help='windows: how many windows the plain per-window loop is timed and checked on')
@@ -388,6 +450,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == 'windows':
         run_windows(args)
+    elif args.workload == 'served':
+        run_served(args)
     else:
         run_ours(args)
 

@@ -79,6 +79,8 @@ class BatchedEngine:
         self.runtime = runtime
         self._foci: dict[Any, GPUFocus] = {}
         self._families: dict[tuple[int, int, int], Filters] = {}
+        self._pairs: dict[tuple[int, int], tuple[GPUFocus, GPUFocus]] = {}
+        self._configs: dict[tuple[int, ...], Config] = {}
 
     def focus(self, focus: Any) -> GPUFocus:
         key = (focus.modulus, focus.rings)
@@ -86,14 +88,33 @@ class BatchedEngine:
             self._foci[key] = GPUFocus(self.runtime, focus)
         return self._foci[key]
 
+    def focus_pair(self, config: Config) -> tuple[GPUFocus, GPUFocus]:
+        """Device focus tables of (A, B): they depend on A and B only (coefficient-adjusted rings)."""
+        key = (config.A, config.B)
+        pair = self._pairs.get(key)
+        if pair is None:
+            af, bf = config.focuses()
+            pair = self._pairs[key] = (self.focus(af), self.focus(bf))
+        return pair
+
+    def config(self, w: 'Window') -> Config:
+        key = (w.p, w.lo, w.hi, w.A, w.B)
+        c = self._configs.get(key)
+        if c is None:
+            if len(self._configs) > 4096:
+                self._configs.clear()
+            c = self._configs[key] = w.config()
+        return c
+
     def family(self, config: Config) -> Filters:
         key = (config.p, config.A, config.B)
         if key not in self._families:
             self._families[key] = Filters(self.runtime, config)
         return self._families[key]
 
-    def plan(self, windows: list[Window], width: int = 100_000_000, tuning: dict[str, int] | None = None,
+    def plan(self, windows: list[Window], width: int | None = 100_000_000, tuning: dict[str, int] | None = None,
              output_cap: int = 1 << 16) -> 'WindowBatch':
+        """Plan a window batch; width None gives every window a single subtile."""
         return WindowBatch(self, windows, width, tuning, output_cap)
 
 
@@ -108,42 +129,45 @@ def _tuning(settings: dict[str, int] | None) -> N.Tuning:
 class WindowBatch:
     """A planned multi-window launch (pc_multi) with its device buffers."""
 
-    def __init__(self, engine: BatchedEngine, windows: list[Window], width: int,
+    def __init__(self, engine: BatchedEngine, windows: list[Window], width: int | None,
                  tuning: dict[str, int] | None, output_cap: int) -> None:
         if not windows:
             raise ValueError('empty window batch')
-        if width <= 0:
+        if width is not None and width <= 0:
             raise ValueError('subtile width must be positive')
         rt = engine.runtime
-        self.runtime, self.engine, self.windows, self.width = rt, engine, list(windows), int(width)
+        self.runtime, self.engine, self.windows = rt, engine, list(windows)
+        self.widths = [int(width) if width is not None else max(1, w.end - w.first) for w in self.windows]
+        self.width = width
         self.output_cap = int(output_cap)
-        self.configs = [w.config() for w in self.windows]
+        self.configs = [engine.config(w) for w in self.windows]
         foci: list[GPUFocus] = []
         families: list[Filters] = []
         index_f: dict[int, int] = {}
         index_m: dict[int, int] = {}
+        self._family_of = []
         spec = (N.Window * len(self.windows))()
         for i, (w, c) in enumerate(zip(self.windows, self.configs)):
             if not 0 <= w.first < w.end <= c.B:
                 raise ValueError('window outside the canonical domain')
-            af, bf = c.focuses()
             ids = []
-            for focus in (af, bf):
-                g = engine.focus(focus)
-                if id(g) not in index_f:
-                    index_f[id(g)] = len(foci)
+            for g in engine.focus_pair(c):
+                k = index_f.get(id(g))
+                if k is None:
+                    k = index_f[id(g)] = len(foci)
                     foci.append(g)
-                ids.append(index_f[id(g)])
+                ids.append(k)
             fam = engine.family(c)
-            if id(fam) not in index_m:
-                index_m[id(fam)] = len(families)
+            m = index_m.get(id(fam))
+            if m is None:
+                m = index_m[id(fam)] = len(families)
                 families.append(fam)
+            self._family_of.append(m)
             s = spec[i]
-            s.first, s.end, s.width = w.first, w.end, self.width
+            s.first, s.end, s.width = w.first, w.end, self.widths[i]
             s.lo0, s.lo1, s.hi0, s.hi1 = c.lo & MASK, c.lo >> 64, c.hi & MASK, c.hi >> 64
-            s.focus_a, s.focus_b, s.family = ids[0], ids[1], index_m[id(fam)]
+            s.focus_a, s.focus_b, s.family = ids[0], ids[1], m
         self.foci, self.families = foci, families
-        self._family_of = [index_m[id(engine.family(c))] for c in self.configs]
         focus_ptrs = (ctypes.c_void_p * len(foci))(*[g.handle.value for g in foci])
         family_ptrs = (ctypes.c_void_p * len(families))(*[f.handle.value for f in families])
         self.tuning = _tuning(tuning)
@@ -208,8 +232,8 @@ class WindowBatch:
             for values in per_tile:
                 values.sort()
             ranges = []
-            for v in range(w.first, w.end, self.width):
-                stop = min(v + self.width, w.end)
+            for v in range(w.first, w.end, self.widths[i]):
+                stop = min(v + self.widths[i], w.end)
                 ranges.append((v, stop, c.u_interval(v)[0], c.u_interval(stop - 1)[1]))
             geo = [(int(a), int(b)) for a, b in geometry[t0:t1]]
             row = batch_result(c, ranges, pops, per_tile, geo, fam.filter_groups, 1 << 62)

@@ -194,13 +194,23 @@ struct PrepArgs {
 // advance linearly (about N_u/N_v < 1 step per row).
 constexpr int PREP_RUN = 16;
 
+// Monotone advance of a bound from its previous position: a few linear steps, then a galloping
+// search (strides 8, 16, 32, ...) that brackets the answer, then a binary search inside the
+// bracket, so a row whose bound moved by g entries costs O(log g) loads near the previous bound.
 __device__ __forceinline__ uint64_t advance_le(const uint64_t *__restrict__ us, uint64_t n, uint64_t B, u128 key,
                                                uint64_t from) {
-    for (int step = 0; step < 16; ++step) {
+    for (int step = 0; step < 4; ++step) {
         if (from >= n || less128(key, mul_wide(__ldg(us + from), B))) return from;
         ++from;
     }
-    return from + count_le(us + from, n - from, B, key);   // long gap: binary search the rest
+    uint64_t lo = from, stride = 8;                      // us[lo - 1] * B <= key
+    for (;;) {
+        const uint64_t probe = lo + stride;
+        if (probe >= n) return lo + count_le(us + lo, n - lo, B, key);
+        if (less128(key, mul_wide(__ldg(us + probe), B))) return lo + count_le(us + lo, probe - lo, B, key);
+        lo = probe + 1;
+        stride *= 2;
+    }
 }
 
 __global__ void k_vprep(const PrepArgs a) {
