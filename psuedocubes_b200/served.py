@@ -42,8 +42,11 @@ A_RINGS = (2, 7, 13, 31, 43, 73, 79, 127, 139, 157, 181)   # the rings of A619, 
 B_RINGS = (9, 19, 37, 61, 67, 97, 103, 109, 151, 163)      # the rings of B619, ascending
 SERVED_PRIMES = (499, 523, 541, 547, 571, 577, 601, 607, 613, 619)
 X_MAX = 3 * 10**27
-#: device seconds per u entry, per v entry and per focused position (measured on the lease path)
-COST_U, COST_V, COST_POSITION = 5e-12, 100e-12, 0.08e-12
+#: device seconds per u entry, per v entry and per focused position.  A u entry costs its window
+#: generation plus its share of the matcher's fixed per-block work (pattern load, residue rows,
+#: barriers: about 30 us of one CTA per 1024-entry block, measured on served steps whose blocks
+#: met ~200 v rows each); a v entry its bounds and pieces; a position its share of the bitset tier.
+COST_U, COST_V, COST_POSITION = 200e-12, 100e-12, 0.08e-12
 U_WINDOW, V_WINDOW, P_WINDOW = 1 << 24, 1 << 22, 2 * 10**10
 STEP_U, STEP_V, STEP_P, STEP_WINDOWS = 1 << 26, 1 << 23, 6 * 10**10, 512
 
