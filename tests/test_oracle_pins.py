@@ -6,6 +6,7 @@ its compiled review tools (focus_window_cpu.cpp, wide.c) and its golden lease re
 from __future__ import annotations
 
 import hashlib
+import os
 import random
 
 import numpy as np
@@ -107,3 +108,37 @@ def test_small_window_edges(oracle, low, high):
     rings = g.rings('A')
     want = [y for y in range(low, high) if all(y % q in r for q, r in rings)]
     assert got == want
+
+
+def test_p67_whole_domain_figures(oracle):
+    """The oracle over 1 < x <= 10^13 at p=67 with A = 2523326, B = 2486169 (v in [0, B) in 64
+    slices): positions, group populations, survivor count and digests (ascending numeric order,
+    and ascending string order as an independent probe recorded it)."""
+    A, B = 2523326, 2486169
+    g = oracle.Geometry(67, 1, 10**13, A, B)
+    fa, fb = oracle.OracleFocus(g, 'A'), oracle.OracleFocus(g, 'B')
+    primes_arr, table = g.residual_arrays()
+    ng = len(g.filter_groups)
+    chunks, positions, groups = [], 0, np.zeros(ng, dtype=np.uint64)
+    step = -(-B // 64)
+    for first in range(0, B, step):
+        end = min(first + step, B)
+        (_, _, ulo, uhi), = g.tile_ranges(first, end, end - first)
+        us, vs = fa.window(ulo, uhi, cap=1 << 40), fb.window(first, end, cap=1 << 40)
+        counts = np.zeros(ng + 3, dtype=np.uint64)
+        cap = 4_000_000
+        out = np.zeros(2 * cap, dtype=np.uint64)
+        assert oracle.lib().oc_masked_batch(us, len(us), vs, len(vs), A, B, 1, 0, 10**13, 0, primes_arr,
+                                            len(g.residuals), table, first, end - first, 1, cap, counts, out,
+                                            os.cpu_count() or 1) == 0
+        n = int(counts[ng + 1])
+        assert n <= cap and not counts[ng + 2]
+        chunks.append(out[:2 * n].reshape(-1, 2)[:, 0].copy())
+        positions += int(counts[0])
+        groups += counts[1:ng + 1]
+    values = np.sort(np.concatenate(chunks))
+    assert positions == 113_117_444 and groups.tolist() == [74_055_342, 66_984_666, 65_848_989]
+    assert len(values) == 65_848_989
+    assert oracle.strings_digest_u64(values) == '55ba793e8e7ad01a69ec2948d21f8ed5167ac7042b6c21394e8519c7924a69f9'
+    full = ('[' + ','.join('"%s"' % s for s in sorted(map(str, values.tolist()))) + ']\n').encode()
+    assert hashlib.sha256(full).hexdigest() == 'f3f1296a795a66e550f16c516d8c752411db58e1b94506b9ff039551ad346587'
