@@ -48,7 +48,7 @@ X_MAX = 3 * 10**27
 #: met ~200 v rows each); a v entry its bounds and pieces; a position its share of the bitset tier.
 COST_U, COST_V, COST_POSITION = 200e-12, 100e-12, 0.08e-12
 U_WINDOW, V_WINDOW, P_WINDOW = 1 << 24, 1 << 22, 2 * 10**10
-STEP_U, STEP_V, STEP_P, STEP_WINDOWS = 1 << 26, 1 << 23, 6 * 10**10, 512
+STEP_U, STEP_V, STEP_P, STEP_WINDOWS = 1 << 27, 1 << 24, 2 * 10**11, 512
 
 
 @dataclass(frozen=True)
