@@ -438,7 +438,10 @@ __device__ __forceinline__ void copy_words(void *dst, const void *src, uint32_t 
 // One lane owns one (v row, u block) piece: it walks the block's K/4 16-byte units in the order
 // (lane + p) mod (K/4), so at every step the 32 lanes of a warp hit each 16-byte bank group
 // exactly 32/(K/4) times whatever rows they read.  Group counters of groups 1..3 live in
-// registers (c[0..2]) and are reduced per subtile when a lane's subtile changes.
+// registers (c[0..2]) and are reduced per subtile when a lane's subtile changes.  The unit loop
+// only marks the units that keep a bit after every bitset filter; once the piece is done, the
+// lanes recompute their marked units and queue the bits, so the warp votes and diverges once per
+// piece instead of after every unit.
 template <int NB, int K, int NT>
 __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     using G = Geo<K>;
@@ -611,7 +614,8 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const uint64_t slot64 = ctile - tile_base;
             const uint32_t meta_hi = (slot64 < SLOT_FAR ? (uint32_t)slot64 : SLOT_FAR) << 12;
 
-#pragma unroll 1
+            uint32_t pend = 0;                            // units of this piece with survivors
+#pragma unroll
             for (uint32_t p = 0; p < U; ++p) {
                 const uint32_t u = (lane + p) & (U - 1);
                 uint4 acc = rows[ro[0] + u];
@@ -635,6 +639,30 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                 }
                 c[0] += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
                 if (c2_live) c[1] += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
+                pend |= (uint32_t)((acc.x | acc.y | acc.z | acc.w) != 0) << p;
+            }
+            while (__any_sync(0xffffffffu, pend != 0)) {      // recompute a marked unit, queue its bits
+                uint4 acc = make_uint4(0, 0, 0, 0);
+                uint32_t u = 0;
+                if (pend) {
+                    const uint32_t p = __ffs(pend) - 1;
+                    pend &= pend - 1;
+                    u = (lane + p) & (U - 1);
+                    acc = rows[ro[0] + u];
+#pragma unroll
+                    for (int f = 1; f < NB; ++f) {
+                        const uint4 w = rows[ro[f] + u];
+                        acc.x &= w.x;
+                        acc.y &= w.y;
+                        acc.z &= w.z;
+                        acc.w &= w.w;
+                    }
+                    if (!full) {
+                        const int32_t lo = s - (int32_t)u * 128, hi = e - (int32_t)u * 128;
+                        acc.x &= unit_mask(lo, hi), acc.y &= unit_mask(lo - 32, hi - 32);
+                        acc.z &= unit_mask(lo - 64, hi - 64), acc.w &= unit_mask(lo - 96, hi - 96);
+                    }
+                }
                 while (__any_sync(0xffffffffu, (acc.x | acc.y | acc.z | acc.w) != 0)) {
                     const bool has = (acc.x | acc.y | acc.z | acc.w) != 0;
                     const uint32_t bal = __ballot_sync(0xffffffffu, has);
