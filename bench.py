@@ -69,6 +69,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            deadline = time.monotonic() + 5.0                 # sampling is running before the timed region
+            while not self.rows and time.monotonic() < deadline:
+                time.sleep(0.02)
         except OSError:
             self.proc = None
         return self
@@ -79,6 +82,9 @@ class ClockSampler:
 
     def __exit__(self, *exc) -> None:
         if self.proc:
+            seen, deadline = len(self.rows), time.monotonic() + 1.0   # one sample after the timed region
+            while len(self.rows) == seen and time.monotonic() < deadline:
+                time.sleep(0.02)
             self.proc.terminate()
             self.proc.wait(timeout=10)
 

@@ -431,6 +431,43 @@ __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bit
     return low_bits((uint32_t)min(max(hi, 0), 32)) & ~low_bits((uint32_t)min(max(lo, 0), 32));
 }
 
+// The unit loop of one (v row, block) piece: AND of the NB rows per 16-byte unit, range masks
+// unless the row covers the whole block (FULL), the group-1 popcount (first four filters) and,
+// when group 2 ends at the last bitset filter (C2), the group-2 popcount.  Returns the mask of
+// units that keep a bit after every bitset filter.
+template <int NB, int U, bool FULL, bool C2>
+__device__ __forceinline__ uint32_t piece_units(const uint4 *__restrict__ rows, const uint32_t (&ro)[NB],
+                                                uint32_t lane, int32_t s, int32_t e, uint32_t (&c)[3]) {
+    uint32_t pend = 0;
+#pragma unroll
+    for (uint32_t p = 0; p < U; ++p) {
+        const uint32_t u = (lane + p) & (U - 1);
+        uint4 acc = rows[ro[0] + u];
+        uint4 acc4;
+#pragma unroll
+        for (int f = 1; f < NB; ++f) {
+            if (f == 4) acc4 = acc;
+            const uint4 w = rows[ro[f] + u];
+            acc.x &= w.x;
+            acc.y &= w.y;
+            acc.z &= w.z;
+            acc.w &= w.w;
+        }
+        if (NB <= 4) acc4 = acc;
+        if (!FULL) {
+            const int32_t lo = s - (int32_t)u * 128, hi = e - (int32_t)u * 128;
+            const uint32_t m0 = unit_mask(lo, hi), m1 = unit_mask(lo - 32, hi - 32);
+            const uint32_t m2 = unit_mask(lo - 64, hi - 64), m3 = unit_mask(lo - 96, hi - 96);
+            acc.x &= m0, acc.y &= m1, acc.z &= m2, acc.w &= m3;
+            acc4.x &= m0, acc4.y &= m1, acc4.z &= m2, acc4.w &= m3;
+        }
+        c[0] += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
+        if (C2) c[1] += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
+        pend |= (uint32_t)((acc.x | acc.y | acc.z | acc.w) != 0) << p;
+    }
+    return pend;
+}
+
 __device__ __forceinline__ void copy_words(void *dst, const void *src, uint32_t bytes) {
     for (uint32_t i = threadIdx.x; i < bytes / 4; i += blockDim.x) ((uint32_t *)dst)[i] = ((const uint32_t *)src)[i];
 }
@@ -614,33 +651,15 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const uint64_t slot64 = ctile - tile_base;
             const uint32_t meta_hi = (slot64 < SLOT_FAR ? (uint32_t)slot64 : SLOT_FAR) << 12;
 
-            uint32_t pend = 0;                            // units of this piece with survivors
-#pragma unroll
-            for (uint32_t p = 0; p < U; ++p) {
-                const uint32_t u = (lane + p) & (U - 1);
-                uint4 acc = rows[ro[0] + u];
-                uint4 acc4;
-#pragma unroll
-                for (int f = 1; f < NB; ++f) {
-                    if (f == 4) acc4 = acc;
-                    const uint4 w = rows[ro[f] + u];
-                    acc.x &= w.x;
-                    acc.y &= w.y;
-                    acc.z &= w.z;
-                    acc.w &= w.w;
-                }
-                if (NB <= 4) acc4 = acc;
-                if (!full) {
-                    const int32_t lo = s - (int32_t)u * 128, hi = e - (int32_t)u * 128;
-                    const uint32_t m0 = unit_mask(lo, hi), m1 = unit_mask(lo - 32, hi - 32);
-                    const uint32_t m2 = unit_mask(lo - 64, hi - 64), m3 = unit_mask(lo - 96, hi - 96);
-                    acc.x &= m0, acc.y &= m1, acc.z &= m2, acc.w &= m3;
-                    acc4.x &= m0, acc4.y &= m1, acc4.z &= m2, acc4.w &= m3;
-                }
-                c[0] += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
-                if (c2_live) c[1] += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
-                pend |= (uint32_t)((acc.x | acc.y | acc.z | acc.w) != 0) << p;
-            }
+            // warp-uniform FULL and block-uniform C2 select the loop body, so the range masks and the
+            // group-2 popcounts are not issued (as predicated code) where they cannot apply
+            uint32_t pend;                                // units of this piece with survivors
+            if (full)
+                pend = c2_live ? piece_units<NB, U, true, true>(rows, ro, lane, s, e, c)
+                               : piece_units<NB, U, true, false>(rows, ro, lane, s, e, c);
+            else
+                pend = c2_live ? piece_units<NB, U, false, true>(rows, ro, lane, s, e, c)
+                               : piece_units<NB, U, false, false>(rows, ro, lane, s, e, c);
             while (__any_sync(0xffffffffu, pend != 0)) {      // recompute a marked unit, queue its bits
                 uint4 acc = make_uint4(0, 0, 0, 0);
                 uint32_t u = 0;
