@@ -204,6 +204,18 @@ int pc_run_plain_static(int device, const uint64_t *us, uint64_t nu, const uint6
                         const uint32_t *primes, uint32_t nres, const uint8_t *allowed, uint64_t *counts,
                         uint64_t *out, uint64_t out_cap, char *err, int err_len);
 
+/*
+ * Canonical JSON of the subtile scopes of consecutive batches, concatenated in batch order: the
+ * bytes a lease transcript hashes (encoded(subtile_scopes) per batch, pseudocube/accounting.py:17-28,
+ * scopes as built at pseudocube/batch_experiment.py:145-157, hashed at pseudocube/optimized.py:61).
+ * Subtiles [first + k width, ...) of [first, end), tiles_per_batch per batch; counts [ntiles x
+ * stride] as pc_run_lease writes them; digests [ntiles x 64] the hex output_sha256 of each subtile.
+ * Host-only; PC_OVERFLOW if cap bytes are too few.
+ */
+int pc_scopes_json(const uint64_t *counts, uint32_t stride, uint32_t ng, uint64_t ntiles, uint64_t first,
+                   uint64_t end, uint64_t width, uint32_t tiles_per_batch, const char *digests, char *out,
+                   uint64_t cap, uint64_t *len);
+
 /* 128-bit limb self-test: for each of n cases (a, b, c, d) in in4, out3 = low, high limb of
  * a*b - c*d mod 2^128 and the borrow flag; replaces the `arithmetic` kernel
  * (kernels/pseudocube.cuh:7-11). */

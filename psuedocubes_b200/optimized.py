@@ -8,12 +8,15 @@ batch order, so the transcript is byte-identical to a batch-by-batch run.
 """
 from __future__ import annotations
 
+import ctypes
 import hashlib
 import time
 from typing import Any, Callable
 
-from .accounting import digest, encoded_scopes
-from .batch_experiment import MaskedMatcher, batch_result, prepare
+import numpy as np
+
+from .accounting import EMPTY_DIGEST, digest, encoded_scopes
+from .batch_experiment import MaskedMatcher, batch_result, prepare, verify_values
 from .focus import Tile
 from .gpu import GPUFocus
 from .multi import validate_result
@@ -119,14 +122,80 @@ def lease_batches(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, first: int
     return out
 
 
+def lease_receipt(matcher: MaskedMatcher, raw: dict[str, Any], first: int, end: int, started: float) -> dict[str, Any]:
+    """The compact receipt of a whole-lease device call, built from its counter arrays: the same
+    fields, sums and transcript bytes as folding every batch result into an Accumulator, with the
+    canonical JSON of the 16,384 subtile scopes written by the library (pc_scopes_json) instead of
+    through 16,384 dicts.  Every emitted value is re-verified on the host as in batch_result."""
+    config, width = matcher.config, PROFILE['tile_width']
+    if not 0 <= first < end or end - first > LEASE_WIDTH:
+        raise ValueError('invalid optimized lease')
+    counts, geometry, per_tile, stats = raw['counts'], raw['geometry'], raw['per_tile'], raw['stats']
+    nt, ng = counts.shape[0], len(matcher.filter_groups)
+    if nt != (end - first + width - 1) // width:
+        raise ValueError('changed arithmetic subtile geometry')
+    if np.any(counts[:, ng + 2]):
+        raise ArithmeticError('unsigned underflow')
+    if np.any(counts[:, ng + 1] > 8192):
+        raise OverflowError('fused tile output overflow; no truncated coverage')
+    verification_started = time.perf_counter()
+    digests = [EMPTY_DIGEST] * nt
+    values: list[int] = []
+    emitted = counts[:, ng + 1].tolist()
+    for t in np.nonzero(counts[:, ng + 1])[0].tolist():
+        tile_values = per_tile[t]
+        lo = first + t * width
+        if len(tile_values) != emitted[t]:
+            raise ArithmeticError('device output count disagrees with its records')
+        if any(not lo <= config.canonical(n)[1] < min(lo + width, end) for n in tile_values):
+            raise ArithmeticError('output assigned to wrong subtile')
+        digests[t] = digest([str(n) for n in tile_values])
+        values.extend(tile_values)
+    if sum(emitted) != len(values):
+        raise ArithmeticError('device output count disagrees with its records')
+    hits = verify_values(config, values)
+    lib = matcher.runtime.lib
+    text = ''.join(digests).encode()
+    cap = nt * (260 + 21 * ng) + 64
+    buf = np.empty(cap, dtype=np.uint8)                  # written by the library, not zeroed first
+    size = ctypes.c_uint64()
+    code = lib.pc_scopes_json(np.ascontiguousarray(counts, dtype=np.uint64).reshape(-1), counts.shape[1], ng, nt, first,
+                              end, width, PROFILE['tiles_per_compute_batch'], text, buf.ctypes.data, cap,
+                              ctypes.byref(size))
+    if code:
+        raise RuntimeError(f'scope encoding failed ({code})')
+    transcript = hashlib.sha256(memoryview(buf)[:size.value]).hexdigest()
+    verification_seconds = time.perf_counter() - verification_started
+    u, v = geometry[:, 0].astype(object), geometry[:, 1].astype(object)
+    strs = [str(n) for n in values]
+    nbatches = (end - first + BATCH_WIDTH - 1) // BATCH_WIDTH
+    row = dict(status='PASS', host_verified=True, receipt_format=PROFILE['receipt_format'],
+               tile_width=width, compute_batch_width=BATCH_WIDTH, compute_batches=nbatches, subtiles_executed=nt,
+               subtile_scopes=[dict(first=str(first), end=str(end), transcript_sha256=transcript,
+                                    output_sha256=digest(strs))],
+               focus_u=int(geometry[:, 0].sum()), focus_v=int(geometry[:, 1].sum()),
+               cartesian_opportunities=int(sum(u * v)), valid_focused_candidates=int(counts[:, 0].sum()),
+               genuine_cubes=len(values) - len(hits), local_survivors=len(values), cube_checks=len(values),
+               kernel_seconds=stats['kernel_ms'] / 1000, focus_enumeration_seconds=stats['window_ms'] / 1000,
+               transfer_seconds=0.0, verification_seconds=verification_seconds,
+               prefilter_build_seconds=stats['bounds_ms'] / 1000,
+               group_survivors=[int(n) for n in counts[:, 1:ng + 1].sum(axis=0)],
+               filter_groups=[list(g) for g in matcher.filter_groups], all_values=strs, cpu_confirmed_hits=hits,
+               overflow_splits=[], elapsed_seconds=time.monotonic() - started,
+               claim='Executed primary coverage; independent arithmetic replay required before any minimum claim.')
+    validate_result(first, end, row)
+    return row
+
+
 def compute_lease(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, first: int, end: int,
                   heartbeat: Callable[[], None] = lambda: None) -> dict[str, Any]:
     started = time.monotonic()
     acc = Accumulator(first, end)
     if hasattr(matcher, 'run_lease'):
-        for start, stop, row in lease_batches(matcher, af, bf, first, end):
-            acc.add(start, stop, row)
-            heartbeat()
+        Tile(first, end).validate(matcher.config)
+        raw = matcher.run_lease(af, bf, first, end, PROFILE['tile_width'])
+        heartbeat()
+        return lease_receipt(matcher, raw, first, end, started)
     else:
         for start in range(first, end, BATCH_WIDTH):
             stop = min(start + BATCH_WIDTH, end)

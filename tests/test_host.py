@@ -167,3 +167,46 @@ def test_scope_encoding_matches_canonical_json():
         assert list(scopes) == [dict(first=str(f), end=str(e), valid_focused_candidates=v, group_survivors=g,
                                      local_survivors=k, output_sha256=d)
                                 for f, e, v, g, k, d in zip(firsts, ends, valid, groups, local, digests)]
+
+
+def test_library_scope_json_equals_canonical_encoding():
+    """pc_scopes_json (host-only, no device) writes, batch after batch, exactly the bytes of
+    encoded(subtile_scopes) that the lease transcript hashes, including a partial last batch and
+    subtile and counters of 2^53 and above."""
+    import ctypes
+    import random
+    from psuedocubes_b200 import _native as N
+    from psuedocubes_b200.accounting import EMPTY_DIGEST, digest, encoded
+    lib = N.lib()
+    rng = random.Random(61)
+    for first, batches, tail, ng in ((575222931200000000, 3, 12345, 24), (0, 1, 0, 3), (10**17, 2, 6_400_000_000 - 1, 1)):
+        width, per = 100_000_000, 64
+        end = first + batches * width * per + tail
+        nt = (end - first + width - 1) // width
+        counts = np.zeros((nt, ng + 3), dtype=np.uint64)
+        top = (1 << 53) + 9
+        for t in range(nt):
+            counts[t, 0] = rng.randrange(0, top)
+            counts[t, 1:ng + 1] = [rng.randrange(0, top if t % 5 == 0 else 10**6) for _ in range(ng)]
+            counts[t, ng + 1] = rng.randrange(0, 3)
+        digests = [EMPTY_DIGEST if counts[t, ng + 1] == 0 else digest([str(t)]) for t in range(nt)]
+        want = b''
+        for b0 in range(first, end, width * per):
+            b1 = min(b0 + width * per, end)
+            scopes = []
+            for v in range(b0, b1, width):
+                t = (v - first) // width
+                scopes.append(dict(first=str(v), end=str(min(v + width, b1)), valid_focused_candidates=int(counts[t, 0]),
+                                   group_survivors=[int(x) for x in counts[t, 1:ng + 1]],
+                                   local_survivors=int(counts[t, ng + 1]), output_sha256=digests[t]))
+            want += encoded(scopes)
+        cap = len(want) + 16
+        buf = ctypes.create_string_buffer(cap)
+        size = ctypes.c_uint64()
+        assert lib.pc_scopes_json(counts.reshape(-1), ng + 3, ng, nt, first, end, width, per, ''.join(digests).encode(),
+                                  ctypes.addressof(buf), cap, ctypes.byref(size)) == 0
+        assert buf.raw[:size.value] == want
+        assert lib.pc_scopes_json(counts.reshape(-1), ng + 3, ng, nt, first, end, width, per, ''.join(digests).encode(),
+                                  ctypes.addressof(buf), len(want) - 1, ctypes.byref(size)) == N.PC_OVERFLOW
+        assert lib.pc_scopes_json(counts.reshape(-1), ng + 3, ng, nt + 1, first, end, width, per,
+                                  ''.join(digests).encode(), ctypes.addressof(buf), cap, ctypes.byref(size)) == N.PC_INVALID
