@@ -209,6 +209,7 @@ def run_ours(args) -> None:
     barrier(dist)
     runtime.synchronize()
     positions, kernel_ms, launches, outputs = 0, 0.0, 0, 0
+    stage_ms = dict(window_ms=0.0, bounds_ms=0.0, kernel_ms=0.0)
     with ClockSampler(local) as clocks:
         runtime.call(lib.pc_mark(ctx, 0))
         for k in range(args.steps):
@@ -217,6 +218,8 @@ def run_ours(args) -> None:
             kernel_ms += st['kernel_ms']
             launches += st['launches']
             outputs += st['outputs']
+            for key in stage_ms:
+                stage_ms[key] += st[key] / args.steps
         runtime.call(lib.pc_mark(ctx, 1))
         elapsed = ctypes.c_double()
         runtime.call(lib.pc_elapsed(ctx, 0, 1, ctypes.byref(elapsed)))
@@ -255,7 +258,7 @@ def run_ours(args) -> None:
                     e2e=dict(value=e2e_positions * world / e2e_seconds if e2e_seconds else None, unit=UNIT, h2d_bytes_per_step=0,
                              d2h_bytes_per_step=int(d2h), api='psuedocubes_b200.optimized.compute_lease'),
                     gpu_launches=launches, clocks=clock, tuning=effective,
-                    kernel_ms_per_step=kernel_ms / args.steps)
+                    kernel_ms_per_step=kernel_ms / args.steps, stage_ms_per_step=stage_ms)
         if world == 1 and not args.no_cpu:
             line['cpu_baseline'] = {k: v for k, v in cpu_sample(1, args.warmup, batches=8).items()
                                     if k in ('value', 'unit', 'cores', 'kind', 'sample')}

@@ -152,60 +152,71 @@ __device__ __forceinline__ void unit_of(const WindowPlan &p, uint64_t words1, ui
     wb = min(p.wb1, wa + WIN_WORDS);
 }
 
-// One warp per window unit of WIN_WORDS = 32 wheel words, one word per lane, so every row load
-// of the warp is one coalesced 128-byte request.  The warp finds its window by a binary search
-// over the windows' first units.  Count pass: per-unit totals.  Emit pass: the lane's exclusive
-// prefix inside the warp, plus the unit's offset inside its window, plus the window's base gives
-// ascending output slots.
+constexpr int WIN_UNITS_PER_WARP = 8;
+
+// One warp per WIN_UNITS_PER_WARP consecutive window units of WIN_WORDS = 32 wheel words each, one
+// word per lane, so every row load of the warp is one coalesced 128-byte request.  The warp finds
+// the window of its first unit by a binary search over the windows' first units and steps to the
+// next window when its units cross into it.  Count pass: per-unit totals.  Emit pass: the lane's
+// exclusive prefix inside the warp, plus the unit's offset inside its window, plus the window's
+// base gives ascending output slots.
 __global__ void k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, const FocusDev *__restrict__ foci,
                           uint64_t units, uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
                           const uint64_t *__restrict__ bases, uint64_t *__restrict__ out) {
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t gu = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    if (gu >= units) return;                            // warp-uniform
-    uint32_t lo = 0, hi = ndesc;                        // last window with unit_base <= gu
+    const uint64_t u0 = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * WIN_UNITS_PER_WARP;
+    if (u0 >= units) return;                            // warp-uniform
+    const uint64_t u1 = umin64(units, u0 + WIN_UNITS_PER_WARP);
+    uint32_t lo = 0, hi = ndesc;                        // last window with unit_base <= u0
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) / 2;
-        if (desc[mid].unit_base <= gu) lo = mid;
+        if (desc[mid].unit_base <= u0) lo = mid;
         else hi = mid;
     }
-    const WindowPlan &p = desc[lo].plan;
-    const uint64_t ubase = desc[lo].unit_base;
-    const FocusDev &f = foci[desc[lo].focus];
-    uint64_t K, wa, wb;
-    unit_of(p, f.words1, gu - ubase, K, wa, wb);
-    const uint64_t w = wa + lane;
-    uint32_t bits = 0;
-    if (w < wb) {
-        bits = 0xffffffffu;
-        for (uint32_t t = 0; t < f.nT; ++t) {
-            const uint32_t s = fastmod32(mod64(K, f.tmq[t]) * f.t_m1mod[t], f.tmq[t].c, f.tq[t]);   // < q^2 < 2^32
-            bits &= __ldg(f.rows + (uint64_t)(f.t_row0[t] + s) * f.words1 + w);
+    uint64_t next_base = lo + 1 < ndesc ? desc[lo + 1].unit_base : UINT64_MAX;
+    for (uint64_t gu = u0; gu < u1; ++gu) {
+        while (gu >= next_base) {                       // the units crossed into the next window
+            ++lo;
+            next_base = lo + 1 < ndesc ? desc[lo + 1].unit_base : UINT64_MAX;
         }
-        const uint64_t jmin = K == p.K0 ? p.j_lo : 0;
-        const uint64_t jmax = K == p.K1 ? p.j_hi : f.count1;
-        const uint64_t j0 = w * 32;
-        if (j0 < jmin) bits &= ~low_bits((uint32_t)(jmin - j0 < 32 ? jmin - j0 : 32));
-        if (j0 + 32 > jmax) bits &= jmax > j0 ? low_bits((uint32_t)(jmax - j0)) : 0u;
-    }
-    const uint32_t n = __popc(bits);
-    if (!offsets) {
-        const uint32_t total = __reduce_add_sync(0xffffffffu, n);
-        if (lane == 0) counts[gu] = total;
-        return;
-    }
-    uint32_t incl = n;
+        const WindowPlan &p = desc[lo].plan;
+        const uint64_t ubase = desc[lo].unit_base;
+        const FocusDev &f = foci[desc[lo].focus];
+        uint64_t K, wa, wb;
+        unit_of(p, f.words1, gu - ubase, K, wa, wb);
+        const uint64_t w = wa + lane;
+        uint32_t bits = 0;
+        if (w < wb) {
+            bits = 0xffffffffu;
+            for (uint32_t t = 0; t < f.nT; ++t) {
+                const uint32_t s = fastmod32(mod64(K, f.tmq[t]) * f.t_m1mod[t], f.tmq[t].c, f.tq[t]);   // < q^2 < 2^32
+                bits &= __ldg(f.rows + (uint64_t)(f.t_row0[t] + s) * f.words1 + w);
+            }
+            const uint64_t jmin = K == p.K0 ? p.j_lo : 0;
+            const uint64_t jmax = K == p.K1 ? p.j_hi : f.count1;
+            const uint64_t j0 = w * 32;
+            if (j0 < jmin) bits &= ~low_bits((uint32_t)(jmin - j0 < 32 ? jmin - j0 : 32));
+            if (j0 + 32 > jmax) bits &= jmax > j0 ? low_bits((uint32_t)(jmax - j0)) : 0u;
+        }
+        const uint32_t n = __popc(bits);
+        if (!offsets) {
+            const uint32_t total = __reduce_add_sync(0xffffffffu, n);
+            if (lane == 0) counts[gu] = total;
+            continue;
+        }
+        uint32_t incl = n;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= (uint32_t)d) incl += y;
-    }
-    uint64_t pos = bases[lo] + (offsets[gu] - offsets[ubase]) + incl - n;
-    const uint64_t base = K * f.M1, j0 = w * 32;
-    while (bits) {
-        const uint32_t b = __ffs(bits) - 1;
-        bits &= bits - 1;
-        out[pos++] = base + __ldg(f.W1 + j0 + b);
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (uint32_t)d) incl += y;
+        }
+        uint64_t pos = bases[lo] + (offsets[gu] - offsets[ubase]) + incl - n;
+        const uint64_t base = K * f.M1, j0 = w * 32;
+        while (bits) {
+            const uint32_t b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            out[pos++] = base + __ldg(f.W1 + j0 + b);
+        }
     }
 }
 
@@ -492,7 +503,8 @@ FocusDev focus_dev(const pc_focus *f) {
 
 int winbatch_count(pc_ctx *ctx, const WinBatch &wb) {
     if (wb.units) {
-        const unsigned grid = (unsigned)((wb.units * 32 + WT - 1) / WT);
+        const uint64_t warps = (wb.units + WIN_UNITS_PER_WARP - 1) / WIN_UNITS_PER_WARP;
+        const unsigned grid = (unsigned)((warps * 32 + WT - 1) / WT);
         k_windows<<<grid, WT, 0, ctx->stream>>>((const WinDesc *)wb.d_desc, wb.n, (const FocusDev *)wb.d_foci, wb.units,
                                                 wb.d_cnt, nullptr, nullptr, nullptr);
         PC_LAUNCHED(ctx, "window count");
@@ -504,7 +516,8 @@ int winbatch_emit(pc_ctx *ctx, const WinBatch &wb, uint64_t *out) {
     if (!wb.out_len) return PC_OK;
     PC_CHECK(ctx, cudaMemsetAsync(out, 0, wb.out_len * 8, ctx->stream));   // padding slots read as 0
     if (wb.units) {
-        const unsigned grid = (unsigned)((wb.units * 32 + WT - 1) / WT);
+        const uint64_t warps = (wb.units + WIN_UNITS_PER_WARP - 1) / WIN_UNITS_PER_WARP;
+        const unsigned grid = (unsigned)((warps * 32 + WT - 1) / WT);
         k_windows<<<grid, WT, 0, ctx->stream>>>((const WinDesc *)wb.d_desc, wb.n, (const FocusDev *)wb.d_foci, wb.units,
                                                 nullptr, wb.d_off, wb.d_base, out);
         PC_LAUNCHED(ctx, "window emit");
