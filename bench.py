@@ -35,9 +35,10 @@ UNIT = 'positions/s'
 BATCHES_TOTAL = 108298517
 LEASE_BATCHES = 256
 OPS_PER_POSITION = 0.53071   # algorithmic 32-bit lane-ops per focused position (3W + 18S1 + 12T + 24Nv)
-# DRAM bytes per focused position of k_match from one ncu capture of a 16-batch lease
-# (36.95 MB over 1.713e10 positions: per-v records and the u list, read once; profiles/)
-DRAM_BYTES_PER_POSITION = 36_952_320 / 17_134_369_251
+# DRAM bytes per focused position of k_match from one ncu capture of a full lease (first seeded
+# lease; dram__bytes_read.sum + dram__bytes_write.sum of the k_match launch: 589,712,640 + 26,647,552
+# bytes over 274,244,194,629 positions; profiles/)
+DRAM_BYTES_PER_POSITION = (589_712_640 + 26_647_552) / 274244194629
 
 
 def seeded_first_batch() -> int:
@@ -251,7 +252,7 @@ def run_ours(args) -> None:
                     roofline=dict(bound='int_alu', achieved=achieved, peak=peak, unit='Tlaneop/s',
                                   frac=achieved / peak if achieved else None,
                                   traffic=DRAM_BYTES_PER_POSITION * positions / args.steps,
-                                  traffic_unit='bytes per launch (ncu capture of a 16-batch lease, scaled by positions)',
+                                  traffic_unit='bytes per launch (ncu capture of a full lease, scaled by positions)',
                                   kernel='k_match (fused bitset + 128-bit filters)',
                                   ops_per_position=OPS_PER_POSITION,
                                   peak_basis=f'{runtime.sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz'),

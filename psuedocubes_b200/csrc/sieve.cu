@@ -102,6 +102,7 @@ struct MatchArgs {
     uint4 *deep;                     // (v lo, v hi, u index, subtile) records
     uint32_t deep_cap;               // records per CTA slice
     uint32_t *deep_count;            // per CTA (may exceed deep_cap: the caller retries larger)
+    unsigned long long *item_next;   // next unclaimed work item (zeroed before the launch)
 };
 
 struct DeepArgs {
@@ -400,6 +401,7 @@ __device__ void build_rows(const uint64_t *__restrict__ us, const FamDev &F, uin
 }
 
 constexpr int CBW = 64;                 // bitmap words per cheap-tier filter (q <= 2047)
+constexpr uint64_t ITEM_GRAB = 2;       // work items a CTA claims at a time
 constexpr int QCAP = 64;                // survivor ring per warp (pending < 64 by construction)
 constexpr uint32_t SLOT_FAR = 0xFFFFF;  // queued slot too large to encode: the drain recomputes it
 
@@ -423,7 +425,7 @@ struct MatchSmem {
         fam = cnt + round16(tmax * (ng + 2) * 4);
         seg = fam + round16(sizeof(FamDev));
         misc = seg + round16(sizeof(SegDev));
-        total = misc + 16;
+        total = misc + 16;                                // deep counter (4 B) and the item grab (8 B at +8)
     }
 };
 
@@ -506,22 +508,32 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
 
     const uint64_t n_items = a.item_prefix[a.nblocks];
     const uint64_t vch = *a.vchunk;
-    const uint64_t i0 = n_items * blockIdx.x / gridDim.x, i1 = n_items * (blockIdx.x + 1) / gridDim.x;
     uint64_t cur = UINT64_MAX, bsearch = 0;
     uint32_t cur_seg = UINT32_MAX, cur_fam = UINT32_MAX;
-    if (i0 < i1) {                                        // block of the first item: last b with prefix[b] <= i0
-        uint64_t lo = 0, hi = a.nblocks;
-        while (hi - lo > 1) {
-            uint64_t mid = (lo + hi) / 2;
-            if (a.item_prefix[mid] <= i0) lo = mid;
-            else hi = mid;
-        }
-        bsearch = lo;
-    }
     const uint32_t nch = a.nch;
+    unsigned long long *grab_s = (unsigned long long *)(base + L.misc + 8);
 
-    for (uint64_t it = i0; it < i1; ++it) {
-        while (a.item_prefix[bsearch + 1] <= it) ++bsearch;  // items are visited in order
+    // Items are handed out in ascending order from one device counter, ITEM_GRAB at a time, so the
+    // CTAs work on neighbouring blocks together: the per-v records of those blocks stay in L2, and
+    // the CTAs finish within one grab of each other.
+    uint64_t it = 0, it_end = 0;
+    for (;;) {
+        if (it == it_end) {
+            __syncthreads();                              // every thread has read the previous grab
+            if (threadIdx.x == 0) *grab_s = atomicAdd(a.item_next, (unsigned long long)ITEM_GRAB);
+            __syncthreads();
+            it = *grab_s;
+            if (it >= n_items) break;
+            it_end = umin64(it + ITEM_GRAB, n_items);
+            uint64_t lo = 0, hi = a.nblocks;              // block of item it: last b with prefix[b] <= it
+            while (hi - lo > 1) {
+                const uint64_t mid = (lo + hi) / 2;
+                if (a.item_prefix[mid] <= it) lo = mid;
+                else hi = mid;
+            }
+            bsearch = lo;
+        }
+        while (a.item_prefix[bsearch + 1] <= it) ++bsearch;  // items of one grab are consecutive
         const uint64_t b = bsearch;
         const uint4 range = a.bv[b];
         const uint64_t va = range.x + (it - a.item_prefix[b]) * vch;
@@ -721,6 +733,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                     atomicAdd((unsigned long long *)&a.counts[tile * a.stride + g], (unsigned long long)cv);
             }
         }
+        ++it;
     }
     __syncthreads();
     if (threadIdx.x == 0) a.deep_count[blockIdx.x] = *deep_ctr;
@@ -1118,6 +1131,7 @@ struct Engine {
     SegDev *d_seg = nullptr;
     FamDev *d_fam = nullptr;
     uint32_t *d_tile_seg = nullptr, *d_blk_seg = nullptr, *d_deep_count = nullptr;
+    unsigned long long *d_item_next = nullptr;
     uint64_t *d_counts = nullptr, *d_geo = nullptr, *d_out = nullptr;
     unsigned long long *d_nout = nullptr;                 // [0] outputs, [1] rows outside the geometry
     VRec *d_rec = nullptr;
@@ -1174,6 +1188,7 @@ int engine_prepare(Engine &E, const pc_tuning *tuning, Scratch &hold) {
     if (!rc) rc = hold.get(&E.d_vchunk, 1);
     if (!rc) rc = hold.get(&E.d_ws, pc_scan_workspace(E.nblocks));
     if (!rc) rc = hold.get(&E.d_deep_count, E.grid);
+    if (!rc) rc = hold.get(&E.d_item_next, 1);
     if (!rc) rc = engine_deep_alloc(E, E.deep_cap);
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
@@ -1206,6 +1221,7 @@ int engine_match(Engine &E, int mode) {
     ma.deep = E.d_deep;
     ma.deep_cap = E.deep_cap;
     ma.deep_count = E.d_deep_count;
+    ma.item_next = E.d_item_next;
     if (E.tn.threads == 1024) return launch_match_n<1024>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
     if (E.tn.threads == 768) return launch_match_n<768>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
     return launch_match_n<512>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
@@ -1218,6 +1234,7 @@ int engine_front(Engine &E, bool events, bool capturing, int *launches) {
     if (E.ntiles) PC_CHECK(ctx, cudaMemsetAsync(E.d_counts, 0, E.ntiles * E.stride * 8, st));
     PC_CHECK(ctx, cudaMemsetAsync(E.d_nout, 0, 16, st));
     PC_CHECK(ctx, cudaMemsetAsync(E.d_deep_count, 0, (uint64_t)E.grid * 4, st));
+    PC_CHECK(ctx, cudaMemsetAsync(E.d_item_next, 0, 8, st));
     if (events) PC_CHECK(ctx, cudaEventRecord(ctx->ev[0], st));
     if (E.nv) {
         PrepArgs pa{};
