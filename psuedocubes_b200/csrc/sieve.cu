@@ -401,7 +401,7 @@ __device__ void build_rows(const uint64_t *__restrict__ us, const FamDev &F, uin
 }
 
 constexpr int CBW = 64;                 // bitmap words per cheap-tier filter (q <= 2047)
-constexpr uint64_t ITEM_GRAB = 2;       // work items a CTA claims at a time
+constexpr uint64_t ITEM_GRAB = 2;       // fewest work items a CTA claims at a time
 constexpr int QCAP = 64;                // survivor ring per warp (pending < 64 by construction)
 constexpr uint32_t SLOT_FAR = 0xFFFFF;  // queued slot too large to encode: the drain recomputes it
 
@@ -513,18 +513,20 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     const uint32_t nch = a.nch;
     unsigned long long *grab_s = (unsigned long long *)(base + L.misc + 8);
 
-    // Items are handed out in ascending order from one device counter, ITEM_GRAB at a time, so the
-    // CTAs work on neighbouring blocks together: the per-v records of those blocks stay in L2, and
-    // the CTAs finish within one grab of each other.
+    // Items are handed out in ascending order from one device counter, so the CTAs work on
+    // neighbouring blocks together: the per-v records of those blocks stay in L2, and the CTAs
+    // finish within one grab of each other.  A grab takes as many items as a block averages (at
+    // least ITEM_GRAB), so a block cut into several items is mostly built by one CTA once.
+    const uint64_t grab = umax64(ITEM_GRAB, n_items / umax64(1, a.nblocks));
     uint64_t it = 0, it_end = 0;
     for (;;) {
         if (it == it_end) {
             __syncthreads();                              // every thread has read the previous grab
-            if (threadIdx.x == 0) *grab_s = atomicAdd(a.item_next, (unsigned long long)ITEM_GRAB);
+            if (threadIdx.x == 0) *grab_s = atomicAdd(a.item_next, (unsigned long long)grab);
             __syncthreads();
             it = *grab_s;
             if (it >= n_items) break;
-            it_end = umin64(it + ITEM_GRAB, n_items);
+            it_end = umin64(it + grab, n_items);
             uint64_t lo = 0, hi = a.nblocks;              // block of item it: last b with prefix[b] <= it
             while (hi - lo > 1) {
                 const uint64_t mid = (lo + hi) / 2;
