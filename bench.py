@@ -173,7 +173,7 @@ def run_ours(args) -> None:
     from psuedocubes_b200.batch_experiment import MaskedMatcher
     from psuedocubes_b200.focus import A619, B619, Config
     from psuedocubes_b200.gpu import GPUFocus, MASK, Runtime
-    from psuedocubes_b200.optimized import PROFILE, compute_lease
+    from psuedocubes_b200.optimized import PROFILE, compute_leases
 
     rank, world, local, dist = dist_setup(args.gpus)
     runtime = Runtime(time.monotonic() + 7200, 16 * 1024**3, 0.5, device=local)
@@ -226,14 +226,14 @@ def run_ours(args) -> None:
         runtime.call(lib.pc_elapsed(ctx, 0, 1, ctypes.byref(elapsed)))
     seconds = max_over_ranks(dist, elapsed.value / 1000, local)
     total_positions = positions * world   # every rank runs the same number of equal-size leases
-    # end to end through the public API: compute_lease with host assembly, verification, transcript
+    # end to end through the public API: compute_leases over consecutive leases (host assembly,
+    # verification and transcript of one lease overlap the device call of the next)
     barrier(dist)
     e2e_steps = args.e2e_steps
     t0 = time.perf_counter()
     e2e_positions = 0
-    for k in range(e2e_steps):
-        first, end = lease_bounds((args.warmup + args.steps + k) * world + rank, args.lease_batches)
-        result = compute_lease(matcher, af, bf, first, end)
+    leases = [lease_bounds((args.warmup + args.steps + k) * world + rank, args.lease_batches) for k in range(e2e_steps)]
+    for result in compute_leases(matcher, af, bf, leases):
         e2e_positions += result['valid_focused_candidates']
     e2e_seconds = max_over_ranks(dist, time.perf_counter() - t0, local) if e2e_steps else 0.0
     d2h = counts.nbytes + geometry.nbytes + 16 + 16 * (outputs // max(1, args.steps))
@@ -257,7 +257,7 @@ def run_ours(args) -> None:
                                   ops_per_position=OPS_PER_POSITION,
                                   peak_basis=f'{runtime.sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz'),
                     e2e=dict(value=e2e_positions * world / e2e_seconds if e2e_seconds else None, unit=UNIT, h2d_bytes_per_step=0,
-                             d2h_bytes_per_step=int(d2h), api='psuedocubes_b200.optimized.compute_lease'),
+                             d2h_bytes_per_step=int(d2h), api='psuedocubes_b200.optimized.compute_leases'),
                     gpu_launches=launches, clocks=clock, tuning=effective,
                     kernel_ms_per_step=kernel_ms / args.steps, stage_ms_per_step=stage_ms)
         if world == 1 and not args.no_cpu:
@@ -442,7 +442,7 @@ def main() -> None:
     parser.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     parser.add_argument('--lease-batches', type=int, default=LEASE_BATCHES,
                         help='batches per step (256 = a full lease; smaller only for profiling)')
-    parser.add_argument('--e2e-steps', type=int, default=2)
+    parser.add_argument('--e2e-steps', type=int, default=8)
     parser.add_argument('--bitset-filters', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--block-words', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--threads', type=int, default=0, help='tuning override (0 = library default)')

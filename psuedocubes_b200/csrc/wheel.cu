@@ -152,12 +152,14 @@ __device__ __forceinline__ void unit_of(const WindowPlan &p, uint64_t words1, ui
     wb = min(p.wb1, wa + WIN_WORDS);
 }
 
-constexpr int WIN_UNITS_PER_WARP = 8;
+constexpr int WIN_UNITS_PER_WARP = 16;
 
 // One warp per WIN_UNITS_PER_WARP consecutive window units of WIN_WORDS = 32 wheel words each, one
 // word per lane, so every row load of the warp is one coalesced 128-byte request.  The warp finds
 // the window of its first unit by a binary search over the windows' first units and steps to the
-// next window when its units cross into it.  Count pass: per-unit totals.  Emit pass: the lane's
+// next window when its units cross into it.  The row addresses of a period are computed once and
+// reused while its units stay in that period (a period spans hundreds of units), and the rows of a
+// unit are loaded together before they are combined.  Count pass: per-unit totals.  Emit pass: the lane's
 // exclusive prefix inside the warp, plus the unit's offset inside its window, plus the window's
 // base gives ascending output slots.
 __global__ void k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, const FocusDev *__restrict__ foci,
@@ -174,6 +176,10 @@ __global__ void k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, cons
         else hi = mid;
     }
     uint64_t next_base = lo + 1 < ndesc ? desc[lo + 1].unit_base : UINT64_MAX;
+    // The rows of period K, kept while consecutive units stay in the same period and window.
+    const uint32_t *row[PC_MAX_WHEEL_T];
+    uint64_t row_K = UINT64_MAX;
+    uint32_t row_win = UINT32_MAX;
     for (uint64_t gu = u0; gu < u1; ++gu) {
         while (gu >= next_base) {                       // the units crossed into the next window
             ++lo;
@@ -186,11 +192,26 @@ __global__ void k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, cons
         unit_of(p, f.words1, gu - ubase, K, wa, wb);
         const uint64_t w = wa + lane;
         uint32_t bits = 0;
+        if (K != row_K || lo != row_win) {             // warp-uniform
+            row_K = K;
+            row_win = lo;
+#pragma unroll
+            for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) {
+                row[t] = f.rows;                        // rows past nT: a valid address, never read
+                if (t < f.nT) {
+                    const uint32_t s = fastmod32(mod64(K, f.tmq[t]) * f.t_m1mod[t], f.tmq[t].c, f.tq[t]);   // < q^2 < 2^32
+                    row[t] += (uint64_t)(f.t_row0[t] + s) * f.words1;
+                }
+            }
+        }
         if (w < wb) {
             bits = 0xffffffffu;
-            for (uint32_t t = 0; t < f.nT; ++t) {
-                const uint32_t s = fastmod32(mod64(K, f.tmq[t]) * f.t_m1mod[t], f.tmq[t].c, f.tq[t]);   // < q^2 < 2^32
-                bits &= __ldg(f.rows + (uint64_t)(f.t_row0[t] + s) * f.words1 + w);
+            if (f.nT) {                                 // all row loads in flight before the first use
+                uint32_t r[PC_MAX_WHEEL_T];
+#pragma unroll
+                for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) r[t] = t < f.nT ? __ldg(row[t] + w) : 0xffffffffu;
+#pragma unroll
+                for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) bits &= r[t];
             }
             const uint64_t jmin = K == p.K0 ? p.j_lo : 0;
             const uint64_t jmax = K == p.K1 ? p.j_hi : f.count1;

@@ -11,7 +11,8 @@ from __future__ import annotations
 import ctypes
 import hashlib
 import time
-from typing import Any, Callable
+from concurrent.futures import Future, ThreadPoolExecutor
+from typing import Any, Callable, Iterable, Iterator, Optional
 
 import numpy as np
 
@@ -203,3 +204,38 @@ def compute_lease(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, first: int
             acc.add(start, stop, matcher.run(batch))
             heartbeat()
     return acc.finish(time.monotonic() - started)
+
+
+def compute_leases(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, leases: Iterable[tuple[int, int]],
+                   heartbeat: Callable[[], None] = lambda: None) -> Iterator[dict[str, Any]]:
+    """Receipts of a sequence of leases, in order, each identical to ``compute_lease`` of it.
+
+    A worker that runs leases back to back overlaps them: the device call of lease k + 1 runs on a
+    helper thread (the library call releases the interpreter lock) while this thread builds and
+    re-verifies the receipt of lease k.  One device call is in flight at a time, so the library
+    context is never used by two threads at once.  Bounds are validated before a lease is issued."""
+    if not hasattr(matcher, 'run_lease'):
+        for first, end in leases:
+            yield compute_lease(matcher, af, bf, first, end, heartbeat)
+        return
+    width = PROFILE['tile_width']
+    pending = iter(leases)
+
+    def issue(pool: ThreadPoolExecutor) -> Optional[tuple[Future, int, int, float]]:
+        lease = next(pending, None)
+        if lease is None:
+            return None
+        first, end = lease
+        if not 0 <= first < end or end - first > LEASE_WIDTH:
+            raise ValueError('invalid optimized lease')
+        Tile(first, end).validate(matcher.config)
+        return pool.submit(matcher.run_lease, af, bf, first, end, width), first, end, time.monotonic()
+
+    with ThreadPoolExecutor(max_workers=1) as pool:
+        current = issue(pool)
+        while current is not None:
+            future, first, end, started = current
+            raw = future.result()
+            heartbeat()
+            current = issue(pool)
+            yield lease_receipt(matcher, raw, first, end, started)

@@ -17,7 +17,7 @@ from psuedocubes_b200 import _native as N
 from psuedocubes_b200.batch_experiment import FusedMatcher, MaskedMatcher, compare, prepare, prepare_arrays
 from psuedocubes_b200.focus import A619, B619, Config, Tile, targeted_coordinates
 from psuedocubes_b200.gpu import DeviceArray, GPUFocus, Matcher
-from psuedocubes_b200.optimized import BATCH_WIDTH, compute_lease
+from psuedocubes_b200.optimized import BATCH_WIDTH, compute_lease, compute_leases
 from psuedocubes_b200.run_production import compute_batch
 
 pytestmark = pytest.mark.gpu
@@ -167,6 +167,24 @@ def test_lease_path_equals_batch_path(runtime, p619, focuses619):
     batchwise = compute_lease(PerBatch(matcher), fa, fb, first, end)
     strip = lambda r: {k: v for k, v in r.items() if not k.endswith('_seconds')}
     assert strip(fused) == strip(batchwise)
+
+
+def test_overlapped_leases_equal_one_by_one(runtime, p619, focuses619):
+    """compute_leases overlaps the device call of the next lease with the receipt of the current
+    one; every receipt must equal compute_lease of the same lease, in the given order."""
+    fa, fb = focuses619
+    gold = golden('golden_lease.json')
+    g0 = int(gold['first'])
+    leases = [(g0, int(gold['end'])), (658625401600000000, 658625401600000000 + 2 * BATCH_WIDTH + 777),
+              (12345, 12345 + BATCH_WIDTH)]
+    matcher = MaskedMatcher(runtime, p619)
+    strip = lambda r: {k: v for k, v in r.items() if not k.endswith('_seconds')}
+    got = [strip(r) for r in compute_leases(matcher, fa, fb, leases)]
+    want = [strip(compute_lease(matcher, fa, fb, first, end)) for first, end in leases]
+    assert got == want
+    assert got[0]['subtile_scopes'][0]['transcript_sha256'] == gold['transcript_sha256']
+    with pytest.raises(ValueError):
+        list(compute_leases(matcher, fa, fb, [(10, 10)]))
 
 
 def test_high_magnitude_canaries(runtime, focuses619):

@@ -210,3 +210,57 @@ def test_library_scope_json_equals_canonical_encoding():
                                   ctypes.addressof(buf), len(want) - 1, ctypes.byref(size)) == N.PC_OVERFLOW
         assert lib.pc_scopes_json(counts.reshape(-1), ng + 3, ng, nt + 1, first, end, width, per,
                                   ''.join(digests).encode(), ctypes.addressof(buf), cap, ctypes.byref(size)) == N.PC_INVALID
+
+
+def test_overlapped_leases_issue_ahead_and_keep_order(p619):
+    """compute_leases issues lease k + 1 to the device before it returns the receipt of lease k,
+    keeps one device call in flight, yields receipts in lease order equal to compute_lease's, and
+    passes a device error through to the caller."""
+    import threading
+    import time
+    import types
+    from psuedocubes_b200.optimized import PROFILE, compute_lease, compute_leases
+    width, fg = PROFILE['tile_width'], p619.filter_groups()
+    ng = len(fg)
+    events, lock, busy = [], threading.Lock(), [0]
+
+    class FakeLeases:
+        config, filter_groups = p619, fg
+        runtime = types.SimpleNamespace(lib=N.lib())
+
+        def run_lease(self, af, bf, first, end, w):
+            with lock:
+                busy[0] += 1
+                assert busy[0] == 1
+                events.append(('run', first))
+            if first == 666:
+                busy[0] -= 1
+                raise ArithmeticError('device failure')
+            nt = (end - first + w - 1) // w
+            counts = np.zeros((nt, ng + 3), dtype=np.uint64)
+            counts[:, 0] = np.arange(nt, dtype=np.uint64) + first % 1000
+            counts[:, 1] = counts[:, 0] // 2
+            geometry = np.ones((nt, 2), dtype=np.uint64)
+            with lock:
+                busy[0] -= 1
+            return dict(counts=counts, geometry=geometry, per_tile=[[] for _ in range(nt)],
+                        stats=dict(kernel_ms=1.0, window_ms=0.5, bounds_ms=0.25))
+
+    leases = [(0, BATCH_WIDTH + 5), (10**17, 10**17 + 3 * width), (5 * BATCH_WIDTH, 6 * BATCH_WIDTH)]
+    got = []
+    for k, receipt in enumerate(compute_leases(FakeLeases(), None, None, leases)):
+        # the generator is suspended here, so the next lease can only run if it was issued already
+        if k + 1 < len(leases):
+            deadline = time.monotonic() + 10
+            while ('run', leases[k + 1][0]) not in events and time.monotonic() < deadline:
+                time.sleep(0.001)
+            assert ('run', leases[k + 1][0]) in events
+        events.append(('receipt', int(receipt['subtile_scopes'][0]['first'])))
+        got.append(receipt)
+    assert [e for e in events if e[0] == 'receipt'] == [('receipt', f) for f, _ in leases]
+    assert [e for e in events if e[0] == 'run'] == [('run', f) for f, _ in leases]
+    strip = lambda r: {k: v for k, v in r.items() if not k.endswith('_seconds')}
+    for (first, end), receipt in zip(leases, got):
+        assert strip(receipt) == strip(compute_lease(FakeLeases(), None, None, first, end))
+    with pytest.raises(ArithmeticError):
+        list(compute_leases(FakeLeases(), None, None, [(0, width), (666, 666 + width)]))
