@@ -433,6 +433,124 @@ def run_served(args) -> None:
         dist.destroy_process_group()
 
 
+CUBE_ROOTS = (1000000001, 1442249570, 619)   # cube roots of (10^27, 3*10^27], tools/check_cpu.py:24-29
+CUBE_METRIC = 'cube roots checked/s (genuine-cube control, p=619, roots of (1e27, 3e27])'
+
+
+def cube_groups(p: int) -> int:
+    """Prime groups of the device sieve (products <= 2^16), as pc_cube_roots forms them."""
+    primes = [q for q in range(2, p + 1) if all(q % d for d in range(2, int(q ** 0.5) + 1))]
+    groups, product = 0, None
+    for q in primes:
+        if product is None or product * q > 1 << 16:
+            groups, product = groups + 1, q
+        else:
+            product *= q
+    return groups
+
+
+def reference_cube_count(first: int, last: int, p: int) -> tuple[int, float]:
+    """The reference's own checker (review/cube_count.c, built into oracle/_ref), one host thread."""
+    exe = ROOT / 'oracle' / '_ref' / 'cube_count'
+    t0 = time.perf_counter()
+    row = json.loads(subprocess.check_output([str(exe), str(first), str(last), str(p)], text=True))
+    return int(row['count']), time.perf_counter() - t0
+
+
+def run_cubes(args) -> None:
+    """The genuine-cube control over the whole p=619 interval: 442,249,570 roots per step."""
+    from psuedocubes_b200 import cubes
+    from psuedocubes_b200.gpu import Runtime
+    rank, world, local, dist = dist_setup(args.gpus)
+    runtime = Runtime(time.monotonic() + 3600, 1 << 30, 0.5, device=local)
+    lib, ctx = runtime.lib, runtime.ctx
+    first, last, p = CUBE_ROOTS
+    n = last - first + 1
+    count, kms = ctypes.c_uint64(), ctypes.c_double()
+
+    def step() -> float:
+        runtime.call(lib.pc_cube_roots(ctx, first, last, p, None, 0, ctypes.byref(count), ctypes.byref(kms)))
+        if count.value != 38322775:
+            raise ArithmeticError(f'genuine-cube control counted {count.value}, want 38322775')
+        return kms.value
+
+    for _ in range(args.warmup):
+        step()
+    barrier(dist)
+    runtime.synchronize()
+    kernel_ms = []
+    with ClockSampler(local) as clocks:
+        runtime.call(lib.pc_mark(ctx, 0))
+        for _ in range(args.steps):
+            kernel_ms.append(step())
+        runtime.call(lib.pc_mark(ctx, 1))
+        elapsed = ctypes.c_double()
+        runtime.call(lib.pc_elapsed(ctx, 0, 1, ctypes.byref(elapsed)))
+    seconds = max_over_ranks(dist, elapsed.value / 1000, local)
+    t0 = time.perf_counter()
+    e2e_steps = max(1, args.e2e_steps)
+    for _ in range(e2e_steps):
+        assert cubes.count_roots(runtime, first, last, p) == 38322775
+    e2e_seconds = max_over_ranks(dist, time.perf_counter() - t0, local)
+    if rank == 0:
+        clock = clocks.summary()
+        sm_mhz = clock['sm_max_mhz'] or 1965.0
+        peak = runtime.sm_count * 4 * 32 * sm_mhz * 1e6 / 1e12
+        groups = cube_groups(p)
+        ops_per_root = 3 * groups / 32     # per (prime group, 32-root word): pattern load, funnel shift, OR
+        mean_ms = statistics.mean(kernel_ms)
+        achieved = ops_per_root * n / (mean_ms / 1000) / 1e12
+        line = dict(metric=CUBE_METRIC, value=n * args.steps * world / seconds, unit='roots/s', n_gpus=world,
+                    steps=args.steps, warmup=args.warmup, ms_per_step=1000 * seconds / args.steps,
+                    higher_is_better=True, scaling='weak', vs_baseline=None, dtype='u32', data='synthetic',
+                    config=dict(workload='genuine-cube control: roots [1000000001, 1442249570] coprime to every '
+                                         'prime <= 619 (tools/check_cpu.py --full-cube-count)',
+                                first=first, last=last, p=p, count=38322775, parallelism=f'replicas{world}',
+                                l2='no input beyond 85 KB of prime patterns per CTA, staged in shared memory (compute bound)'),
+                    roofline=dict(bound='int_alu', achieved=achieved, peak=peak, unit='Tlaneop/s', frac=achieved / peak,
+                                  traffic=None, kernel='k_roots (count)', ops_per_root=ops_per_root, prime_groups=groups,
+                                  kernel_ms=mean_ms,
+                                  peak_basis=f'{runtime.sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz'),
+                    e2e=dict(value=n * e2e_steps * world / e2e_seconds, unit='roots/s', h2d_bytes_per_step=0,
+                             d2h_bytes_per_step=8, api='psuedocubes_b200.cubes.count_roots'),
+                    gpu_launches=args.steps, clocks=clock)
+        if world == 1 and not args.no_cpu:
+            ref_count, ref_seconds = reference_cube_count(first, last, p)
+            assert ref_count == 38322775
+            line['cpu_baseline'] = dict(value=n / ref_seconds, unit='roots/s', cores=1, kind='reference',
+                                        sample='the whole interval, 442,249,570 roots, review/cube_count.c '
+                                               '(built from the reference sources into oracle/_ref)')
+        print(json.dumps(line), flush=True)
+    runtime.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_reference_cubes(args) -> None:
+    rank, world, local, dist = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    first, last, p = CUBE_ROOTS
+    n = last - first + 1
+    for _ in range(max(0, min(args.warmup, 1))):
+        reference_cube_count(first, first + 10**7, p)
+    seconds = 0.0
+    for _ in range(args.steps):
+        count, t = reference_cube_count(first, last, p)
+        assert count == 38322775
+        seconds += t
+    value = n * args.steps / seconds
+    line = dict(metric=CUBE_METRIC, value=value, unit='roots/s', n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                ms_per_step=1000 * seconds / args.steps, higher_is_better=True, scaling='weak', vs_baseline=None,
+                dtype='u32', data='synthetic', impl='reference',
+                config=dict(workload='genuine-cube control: roots [1000000001, 1442249570] coprime to every prime <= 619',
+                            first=first, last=last, p=p, count=38322775),
+                cpu_baseline=dict(value=value, unit='roots/s', cores=1, kind='reference',
+                                  sample='the whole interval per step, review/cube_count.c (oracle/_ref)'),
+                e2e=dict(value=value, unit='roots/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument('--gpus', type=int, default=1)
@@ -446,9 +564,10 @@ def main() -> None:
     parser.add_argument('--bitset-filters', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--block-words', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--threads', type=int, default=0, help='tuning override (0 = library default)')
-    parser.add_argument('--workload', choices=('lease', 'windows', 'served'), default='lease',
+    parser.add_argument('--workload', choices=('lease', 'windows', 'served', 'cubes'), default='lease',
                         help='lease: the p=619 production lease (headline); windows: 512 uneven windows; '
-                             'served: Poisson range-certification requests')
+                             'served: Poisson range-certification requests; cubes: the genuine-cube control '
+                             'over the whole p=619 interval')
     parser.add_argument('--requests', type=int, default=100, help='served: requests in the arrival stream')
     parser.add_argument('--served-limit', type=float, default=240.0, help='served: seconds before the loop stops')
     parser.add_argument('--plain-limit', type=float, default=60.0, help='served: seconds for the plain loop')
@@ -456,8 +575,12 @@ def main() -> None:
     parser.add_argument('--plain-windows', type=int, default=64,
                         help='windows: how many windows the plain per-window loop is timed and checked on')
     args = parser.parse_args()
-    if args.impl == 'reference':
+    if args.impl == 'reference' and args.workload == 'cubes':
+        run_reference_cubes(args)
+    elif args.impl == 'reference':
         run_reference(args)
+    elif args.workload == 'cubes':
+        run_cubes(args)
     elif args.workload == 'windows':
         run_windows(args)
     elif args.workload == 'served':

@@ -216,6 +216,18 @@ int pc_scopes_json(const uint64_t *counts, uint32_t stride, uint32_t ng, uint64_
                    uint64_t end, uint64_t width, uint32_t tiles_per_batch, const char *digests, char *out,
                    uint64_t cap, uint64_t *len);
 
+/*
+ * Genuine-cube control: the number of integers a in [first, last] coprime to every prime <= p,
+ * i.e. the cube roots whose cubes a correct sieve of bound p must emit.  Replaces the reference's
+ * host checkers review/cube_count.c:12-37 and review/cube_count_independent.c:9-34 (same inclusive
+ * root bounds and limits: 1 <= first <= last < 2^32, 2 <= p <= 2000, else PC_INVALID).  With
+ * roots == NULL only *count is written; otherwise the roots are also written to roots[cap] on the
+ * host in ascending order (their --list form), or PC_OVERFLOW is returned with *count set when
+ * more than cap exist.  kernel_ms (may be NULL) receives the device time of the sieve launches.
+ */
+int pc_cube_roots(pc_ctx *ctx, uint64_t first, uint64_t last, uint32_t p, uint32_t *roots, uint64_t cap,
+                  uint64_t *count, double *kernel_ms);
+
 /* 128-bit limb self-test: for each of n cases (a, b, c, d) in in4, out3 = low, high limb of
  * a*b - c*d mod 2^128 and the borrow flag; replaces the `arithmetic` kernel
  * (kernels/pseudocube.cuh:7-11). */

@@ -210,7 +210,25 @@ def lib() -> ctypes.CDLL:
                                  _U32P, u32, _U8P, u64, _U64P, _U64P]
     so.oc_json_strings_u64.argtypes = [_U64P, u64, ctypes.c_char_p, u64]
     so.oc_json_strings_u64.restype = u64
+    so.oc_cube_roots.argtypes = [u64, u64, u32, ctypes.c_void_p, u64, ctypes.POINTER(u64), ctypes.c_int]
     return so
+
+
+def cube_roots(first: int, last: int, p: int, listed: bool = False, threads: int = 1) -> Any:
+    """Roots a in [first, last] coprime to every prime <= p (review/cube_count.c:12-37): the
+    count, or with ``listed`` the ascending roots as a uint32 array."""
+    count = ctypes.c_uint64()
+    if not listed:
+        rc = lib().oc_cube_roots(first, last, p, None, 0, ctypes.byref(count), threads)
+        if rc:
+            raise ValueError(f'oracle cube roots rejected ({rc})')
+        return count.value
+    cap = last - first + 1 if 1 <= first <= last else 0
+    out = np.zeros(max(1, cap), dtype=np.uint32)
+    rc = lib().oc_cube_roots(first, last, p, out.ctypes.data, cap, ctypes.byref(count), 1)
+    if rc:
+        raise ValueError(f'oracle cube roots rejected ({rc})')
+    return out[:count.value]
 
 
 def wide(cases: np.ndarray) -> np.ndarray:

@@ -15,6 +15,8 @@
  *                   later filters with group counters every four filters (:222-228), per-subtile
  *                   counters and output slots (:206-207, :229-230).
  *   oc_wide         review/wide.c:3-7 (a*b - c*d mod 2^128 and the borrow flag).
+ *   oc_cube_roots   review/cube_count.c:12-37: the roots in [first, last] coprime to every prime
+ *                   <= p, by a segmented byte sieve (count, and the ascending list up to cap).
  *
  * Per-subtile counter layout (as the reference's fused kernel): ng+3 uint64 per subtile,
  * [0] focused positions, [1..ng] group survivors, [ng+1] outputs, [ng+2] underflows.
@@ -361,4 +363,77 @@ uint64_t oc_json_strings_u64(const uint64_t *vals, uint64_t n, char *buf, uint64
     buf[pos++] = ']';
     buf[pos++] = '\n';
     return pos;
+}
+
+/* ---- genuine-cube control (review/cube_count.c:12-37) ---------------------------------- */
+
+typedef struct {
+    uint64_t first, last, count;
+    const uint32_t *primes;
+    uint32_t np;
+    uint32_t *roots;      /* NULL: count only */
+    uint64_t cap;
+} roots_job;
+
+static void *roots_slice(void *arg) {
+    roots_job *j = (roots_job *)arg;
+    enum { SEGMENT = 1 << 20 };
+    unsigned char *keep = malloc(SEGMENT);
+    if (!keep) { j->count = UINT64_MAX; return NULL; }
+    for (uint64_t start = j->first; start <= j->last;) {
+        uint64_t n = j->last - start + 1;
+        if (n > SEGMENT) n = SEGMENT;
+        memset(keep, 1, n);
+        for (uint32_t i = 0; i < j->np; ++i) {
+            uint64_t q = j->primes[i], m = (start + q - 1) / q * q;   /* first multiple >= start */
+            for (; m < start + n; m += q) keep[m - start] = 0;
+        }
+        for (uint64_t i = 0; i < n; ++i)
+            if (keep[i]) {
+                if (j->roots && j->count < j->cap) j->roots[j->count] = (uint32_t)(start + i);
+                j->count++;
+            }
+        start += n;
+    }
+    free(keep);
+    return NULL;
+}
+
+/* Returns 2 on invalid bounds (as the reference checker's exit status), 1 when a list was asked
+ * for and more than cap roots exist (count still set), else 0.  threads > 1 splits a count-only
+ * range into contiguous slices. */
+int oc_cube_roots(uint64_t first, uint64_t last, uint32_t p, uint32_t *roots, uint64_t cap, uint64_t *count,
+                  int threads) {
+    if (first < 1 || last < first || last > UINT32_MAX || p < 2 || p > 2000) return 2;
+    uint32_t primes[400], np = 0;
+    for (uint32_t q = 2; q <= p; ++q) {
+        int prime = 1;
+        for (uint32_t d = 2; d * d <= q; ++d)
+            if (q % d == 0) { prime = 0; break; }
+        if (prime) primes[np++] = q;
+    }
+    if (roots || threads < 1) threads = 1;
+    if (threads > 64) threads = 64;
+    roots_job jobs[64];
+    pthread_t tid[64];
+    const uint64_t n = last - first + 1, per = (n + threads - 1) / threads;
+    int started = 0;
+    for (int t = 0; t < threads; ++t) {
+        const uint64_t a = first + (uint64_t)t * per;
+        if (a > last) break;
+        jobs[t] = (roots_job){a, (last - a < per ? last : a + per - 1), 0, primes, np, roots, cap};
+        if (threads == 1) roots_slice(&jobs[t]);
+        else pthread_create(&tid[t], NULL, roots_slice, &jobs[t]);
+        started++;
+    }
+    uint64_t total = 0;
+    int failed = 0;
+    for (int t = 0; t < started; ++t) {
+        if (threads > 1) pthread_join(tid[t], NULL);
+        if (jobs[t].count == UINT64_MAX) failed = 1;
+        else total += jobs[t].count;
+    }
+    if (failed) return 3;
+    *count = total;
+    return roots && total > cap ? 1 : 0;
 }

@@ -10,7 +10,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / 'csrc'
 OUT = HERE / '_lib' / 'libpcube.so'
-SOURCES = ('runtime.cu', 'wheel.cu', 'sieve.cu', 'receipt.cu')
+SOURCES = ('runtime.cu', 'wheel.cu', 'sieve.cu', 'receipt.cu', 'cubes.cu')
 FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-lineinfo', '-O3', '-std=c++17',
          '-Xcompiler', '-fPIC', '-shared', '--expt-relaxed-constexpr']
 

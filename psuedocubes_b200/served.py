@@ -17,6 +17,8 @@ all admitted requests, smallest remaining work first, into one multi-window laun
 shares the device.  Requests are admitted in arrival order while the device memory they reserve
 (their focus tables and output buffers) fits the cap; focus tables and filter families stay
 resident across requests.  The host verifies one step's outputs while the device runs the next.
+Every finished request is checked against the device genuine-cube control (``cubes``): the cubes
+it emitted must be exactly the cubes a^3 in (x_lo, x_hi] with a coprime to every prime <= p.
 ``plain_loop`` is the sequential plain per-request loop of the same build (the reference's plain
 tile matcher, one request after another) used as the baseline.
 """
@@ -33,6 +35,7 @@ from typing import Any
 import numpy as np
 
 from .batched import BatchedEngine, Window
+from .cubes import genuine_cube_count
 from .focus import Config, Tile
 from .gpu import Matcher, Runtime
 from .tables import allowed
@@ -149,6 +152,7 @@ class Work:
     windows: int = 0
     admitted: float = 0.0
     reserved: int = 0
+    control: Future | None = None    # the device genuine-cube count of the request
 
 
 def request_windows(req: Request, plan: Plan) -> list[tuple[Window, float]]:
@@ -268,6 +272,10 @@ class ServedLoop:
             tables += min(256 << 20, 8 * count + (1 << 20))
         return tables + (16 << 20)
 
+    def _control(self, req: Request) -> int:
+        """The genuine cubes (x_lo, x_hi] must hold at bound p, counted on the device."""
+        return genuine_cube_count(self.runtime, req.p, req.lo, req.hi)
+
     def _device_step(self, windows: list[Window]) -> tuple[np.ndarray, np.ndarray, dict[str, Any], list[int]]:
         """One multi-window launch (one subtile per window).  A step whose outputs overflow the
         output buffer is split in halves and rerun; counters of an overflowed run are complete, but
@@ -330,6 +338,8 @@ class ServedLoop:
                 w.remaining = sum(p for _, p in w.pending)
                 w.groups = [0] * len(w.config.filter_groups())
                 w.admitted, w.reserved = clock(), need
+                # the genuine-cube control runs on the device thread ahead of the request's steps
+                w.control = pool.submit(self._control, r)
                 self.reserved += need
                 active.append(w)
 
@@ -380,6 +390,10 @@ class ServedLoop:
                 active.remove(w)
                 self.reserved -= w.reserved
                 res = _finish(w)
+                res['cube_control'] = w.control.result()
+                if res['cube_control'] != res['genuine_cubes']:
+                    raise ArithmeticError(f'request {w.request.id}: {res["genuine_cubes"]} genuine cubes emitted, '
+                                          f'the device control counts {res["cube_control"]}')
                 res['arrival'] = w.request.arrival
                 res['latency'] = clock() - w.request.arrival if realtime else None
                 results[w.request.id] = res

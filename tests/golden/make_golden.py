@@ -3,6 +3,7 @@
 Run from the repository root in a container where the reference tree is mounted:
 
     python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py /root/reference --cube-roots-only    # cube_roots.json alone
 
 It imports the reference's own Python (pseudocube.focus / oracle / tables / accounting,
 review.verify_cube) from a scratch copy, runs the reference's compiled review tools from
@@ -29,6 +30,44 @@ ROOT = HERE.parents[1]
 def dump(name: str, value: object) -> None:
     (HERE / name).write_text(json.dumps(value, indent=1, sort_keys=True) + '\n')
     print('wrote', name)
+
+
+def cube_root_fixtures(reference: Path) -> None:
+    """Genuine-cube control: the reference's recorded full-interval count
+    (results/completion-2026-09-16/cube_count*.json) and its two compiled checkers
+    (review/cube_count.c, review/cube_count_independent.c, built into oracle/_ref) on list and
+    count cases; the two checkers must agree on every case."""
+    import subprocess
+
+    def run(name: str, a: int, b: int, p: int, listed: bool) -> dict:
+        cmd = [str(ROOT / 'oracle/_ref' / name), str(a), str(b), str(p)] + (['--list'] if listed else [])
+        return json.loads(subprocess.check_output(cmd, text=True))
+
+    recorded = []
+    for name in ('cube_count', 'cube_count_independent'):
+        row = json.loads((reference / f'results/completion-2026-09-16/{name}.json').read_text())
+        recorded.append(dict(checker=name, algorithm=row['algorithm'], first=int(row['root_first']),
+                             last=int(row['root_last']), p=int(row['p']), count=int(row['count']),
+                             source=f'results/completion-2026-09-16/{name}.json'))
+    listed = []
+    for a, b, p in ((1, 1000, 7), (1, 1000, 2), (1, 1000, 3), (2, 2, 2), (1, 1, 2000), (1, 100000, 619),
+                    (1000000001, 1000100000, 619), (1442149571, 1442249570, 619), (4294867296, 4294967295, 619),
+                    (999999937, 1000099936, 1999), (3, 34, 31)):
+        rows = [run(name, a, b, p, True) for name in ('cube_count', 'cube_count_independent')]
+        assert rows[0]['roots'] == rows[1]['roots'] and rows[0]['count'] == rows[1]['count']
+        roots = rows[0]['roots']
+        listed.append(dict(first=a, last=b, p=p, count=int(rows[0]['count']), head=[int(x) for x in roots[:16]],
+                           tail=[int(x) for x in roots[-16:]],
+                           sha256=hashlib.sha256(','.join(roots).encode()).hexdigest()))
+    counted = []
+    for a, b, p in ((1, 10**7, 619), (123456789, 133456789, 1999), (4000000000, 4294967295, 619),
+                    (1, 4294967295, 2), (1000000001, 1442249570, 5), (1000000001, 1442249570, 97),
+                    (1000000001, 1442249570, 2000), (7, 7, 5), (1, 2**20 + 17, 619)):
+        rows = [run(name, a, b, p, False) for name in ('cube_count', 'cube_count_independent')]
+        assert rows[0]['count'] == rows[1]['count']
+        counted.append(dict(first=a, last=b, p=p, count=int(rows[0]['count'])))
+    dump('cube_roots.json', dict(recorded=recorded, listed=listed, counted=counted,
+                                 list_digest='sha256 of the ascending decimal roots joined by commas'))
 
 
 def main(reference: Path) -> None:
@@ -192,7 +231,13 @@ def main(reference: Path) -> None:
                              allowed_31=list(allowed(31)), allowed_9=list(allowed(9))))
     shutil.rmtree(scratch)
     _ = encoded
+    cube_root_fixtures(reference)
 
 
 if __name__ == '__main__':
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else '/root/reference'))
+    args = [a for a in sys.argv[1:] if not a.startswith('--')]
+    ref = Path(args[0] if args else '/root/reference')
+    if '--cube-roots-only' in sys.argv:
+        cube_root_fixtures(ref)
+    else:
+        main(ref)

@@ -103,7 +103,10 @@ class _FakeLoop:
                 return counts, np.zeros((0, 2), dtype=np.uint64), dict(kernel_ms=0.1, total_ms=0.2), \
                     [len(w.config().filter_groups()) for w in windows]
 
-        Loop.seen = []
+            def _control(self, req):
+                return Loop.control
+
+        Loop.seen, Loop.control = [], 0
         return Loop(runtime=None, memory_cap=memory_cap)
 
 
@@ -119,4 +122,9 @@ def test_scheduler_runs_every_window_once():
             plan = plan_request(r.p, r.lo, r.hi)
             total = sum(w.end - w.first for w, _ in request_windows(r, plan))
             assert run['results'][r.id]['valid_focused_candidates'] == total
+            assert run['results'][r.id]['cube_control'] == 0
         assert loop.reserved == 0
+    loop = _FakeLoop.make()
+    type(loop).control = 1                           # a control that disagrees with what was emitted
+    with pytest.raises(ArithmeticError):
+        loop.run(reqs[:1], realtime=False)
