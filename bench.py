@@ -226,8 +226,9 @@ def run_ours(args) -> None:
         runtime.call(lib.pc_elapsed(ctx, 0, 1, ctypes.byref(elapsed)))
     seconds = max_over_ranks(dist, elapsed.value / 1000, local)
     total_positions = positions * world   # every rank runs the same number of equal-size leases
-    # end to end through the public API: compute_leases over consecutive leases (host assembly,
-    # verification and transcript of one lease overlap the device call of the next)
+    # end to end through the public API: compute_leases over consecutive leases (the device runs
+    # them back to back in the library's lease loop; host assembly, verification and transcript of
+    # each lease overlap the device work of the next)
     barrier(dist)
     e2e_steps = args.e2e_steps
     t0 = time.perf_counter()
@@ -560,7 +561,7 @@ def main() -> None:
     parser.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     parser.add_argument('--lease-batches', type=int, default=LEASE_BATCHES,
                         help='batches per step (256 = a full lease; smaller only for profiling)')
-    parser.add_argument('--e2e-steps', type=int, default=8)
+    parser.add_argument('--e2e-steps', type=int, default=16)
     parser.add_argument('--bitset-filters', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--block-words', type=int, default=0, help='tuning override (0 = library default)')
     parser.add_argument('--threads', type=int, default=0, help='tuning override (0 = library default)')

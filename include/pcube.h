@@ -136,6 +136,20 @@ int pc_run_lease(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb, const pc_f
                  uint64_t *counts, uint64_t *geometry, uint64_t *out, uint64_t out_cap, uint64_t *n_out,
                  pc_stats *stats);
 
+/*
+ * pc_run_lease over leases [first[i], end[i]), i < n, one after another on the calling thread,
+ * each with its own counts[i], geometry[i] and out[i] (out_cap records) as pc_run_lease.  status[i]
+ * is set to 1 + the lease's return code once its results are on the host (a release store), so a
+ * second host thread may consume lease i while later leases run; the call stops at, and returns the
+ * code of, the first lease that fails.  stats may be NULL.  A worker that commits lease after lease
+ * (pseudocube/multi.py:197-272) calls this from a helper thread instead of compute_lease per lease.
+ */
+int pc_run_leases(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb, const pc_filters *filters,
+                  const pc_tuning *tuning, uint32_t n, const uint64_t *first, const uint64_t *end, uint64_t width,
+                  uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1, uint64_t *const *counts,
+                  uint64_t *const *geometry, uint64_t *const *out, uint64_t out_cap, uint64_t *n_out,
+                  pc_stats *stats, int32_t *status);
+
 /* Flags of pc_multi_run. */
 #define PC_RUN_GRAPH 1u   /* record the run into a CUDA graph once, then replay it on every call */
 

@@ -24,7 +24,7 @@ PC_OK, PC_OVERFLOW, PC_INVALID, PC_ARITHMETIC, PC_TIMEOUT, PC_NOMEM, PC_CUDA = r
 SYMBOLS = ('pc_version', 'pc_device_count', 'pc_last_error', 'pc_init', 'pc_free', 'pc_mem_info',
            'pc_device_info', 'pc_sync', 'pc_mark', 'pc_elapsed', 'pc_buf_upload', 'pc_buf_download', 'pc_buf_size', 'pc_buf_free',
            'pc_buf_searchsorted', 'pc_focus_create', 'pc_focus_free', 'pc_focus_info', 'pc_focus_window',
-           'pc_filters_create', 'pc_filters_free', 'pc_run_batch', 'pc_run_lease', 'pc_multi_create',
+           'pc_filters_create', 'pc_filters_free', 'pc_run_batch', 'pc_run_lease', 'pc_run_leases', 'pc_multi_create',
            'pc_multi_run', 'pc_multi_layout', 'pc_multi_results', 'pc_multi_free', 'pc_run_plain',
            'pc_run_plain_static', 'pc_scopes_json', 'pc_cube_roots', 'pc_selftest_wide')
 
@@ -114,6 +114,9 @@ def lib() -> ctypes.CDLL:
                                        _U32P, _U32, _U8P, _U64P, _U64P, _U64, ctypes.c_char_p, ctypes.c_int]
     so.pc_scopes_json.argtypes = [_U64P, _U32, _U32, _U64, _U64, _U64, _U64, _U32, ctypes.c_char_p, ctypes.c_void_p,
                                   _U64, ctypes.POINTER(_U64)]
+    so.pc_run_leases.argtypes = [_P, _P, _P, _P, ctypes.POINTER(Tuning), _U32, _U64P, _U64P, _U64, _U64, _U64, _U64, _U64,
+                                 pp, pp, pp, _U64, _U64P, ctypes.POINTER(Stats),
+                                 np.ctypeslib.ndpointer(dtype=np.int32, flags='C_CONTIGUOUS')]
     so.pc_cube_roots.argtypes = [_P, _U64, _U64, _U32, ctypes.c_void_p, _U64, ctypes.POINTER(_U64),
                                  ctypes.POINTER(ctypes.c_double)]
     so.pc_selftest_wide.argtypes = [_P, _U64P, _U64P, _U64]

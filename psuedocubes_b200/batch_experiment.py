@@ -97,8 +97,8 @@ def split_outputs(records: np.ndarray, ntiles: int) -> list[list[int]]:
         tile = (records[:, 1] >> np.uint64(32)).astype(np.int64)
         for t, a, b in zip(tile.tolist(), lo.tolist(), hi.tolist()):
             per[t].append(a | (b << 64))
-        for values in per:
-            values.sort()
+        for t in set(tile.tolist()):
+            per[t].sort()
     return per
 
 

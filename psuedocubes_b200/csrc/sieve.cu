@@ -1498,6 +1498,26 @@ extern "C" int pc_run_lease(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb,
     return rc;
 }
 
+// Leases one after another on the calling thread, so a host runtime that holds a lock while it
+// builds receipts (an interpreter) never sits between two device calls.  status[i] becomes
+// 1 + the return code of lease i once its outputs are on the host (release order), so another
+// thread can consume lease i while later leases run; the loop stops at the first failing lease.
+extern "C" int pc_run_leases(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb, const pc_filters *f,
+                             const pc_tuning *tuning, uint32_t n, const uint64_t *first, const uint64_t *end,
+                             uint64_t width, uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1,
+                             uint64_t *const *counts, uint64_t *const *geometry, uint64_t *const *out, uint64_t out_cap,
+                             uint64_t *n_out, pc_stats *stats, int32_t *status) {
+    if (!ctx || (n && (!first || !end || !counts || !geometry || !out || !n_out || !status)))
+        return pc_fail(ctx, PC_INVALID, "invalid lease list");
+    for (uint32_t i = 0; i < n; ++i) {
+        const int rc = pc_run_lease(ctx, fa, fb, f, tuning, first[i], end[i], width, lo0, lo1, hi0, hi1, counts[i],
+                                    geometry[i], out[i], out_cap, n_out + i, stats ? stats + i : nullptr);
+        __atomic_store_n(status + i, rc + 1, __ATOMIC_RELEASE);
+        if (rc) return rc;
+    }
+    return PC_OK;
+}
+
 extern "C" int pc_run_plain(pc_ctx *ctx, const pc_filters *f, const pc_buf *us, uint64_t u_off, uint64_t nu,
                             const pc_buf *vs, uint64_t v_off, uint64_t nv, uint64_t lo0, uint64_t lo1, uint64_t hi0,
                             uint64_t hi1, uint64_t *counts, uint64_t *out, uint64_t out_cap, pc_stats *stats) {

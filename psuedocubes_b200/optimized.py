@@ -11,15 +11,17 @@ from __future__ import annotations
 import ctypes
 import hashlib
 import time
+from collections import deque
 from concurrent.futures import Future, ThreadPoolExecutor
-from typing import Any, Callable, Iterable, Iterator, Optional
+from typing import Any, Callable, Iterable, Iterator
 
 import numpy as np
 
 from .accounting import EMPTY_DIGEST, digest, encoded_scopes
-from .batch_experiment import MaskedMatcher, batch_result, prepare, verify_values
+from . import _native as N
+from .batch_experiment import MaskedMatcher, batch_result, prepare, split_outputs, verify_values
 from .focus import Tile
-from .gpu import GPUFocus
+from .gpu import MASK, GPUFocus
 from .multi import validate_result
 
 PROFILE: dict[str, Any] = dict(engine='residue-bitset-batch-v1', tile_width=100_000_000,
@@ -167,7 +169,11 @@ def lease_receipt(matcher: MaskedMatcher, raw: dict[str, Any], first: int, end: 
         raise RuntimeError(f'scope encoding failed ({code})')
     transcript = hashlib.sha256(memoryview(buf)[:size.value]).hexdigest()
     verification_seconds = time.perf_counter() - verification_started
-    u, v = geometry[:, 0].astype(object), geometry[:, 1].astype(object)
+    gu, gv = geometry[:, 0], geometry[:, 1]
+    if nt and int(gu.max()) * int(gv.max()) * nt < 1 << 64:      # the uint64 sum is exact
+        cartesian = int((gu * gv).sum())
+    else:
+        cartesian = int(sum(gu.astype(object) * gv.astype(object)))
     strs = [str(n) for n in values]
     nbatches = (end - first + BATCH_WIDTH - 1) // BATCH_WIDTH
     row = dict(status='PASS', host_verified=True, receipt_format=PROFILE['receipt_format'],
@@ -175,7 +181,7 @@ def lease_receipt(matcher: MaskedMatcher, raw: dict[str, Any], first: int, end: 
                subtile_scopes=[dict(first=str(first), end=str(end), transcript_sha256=transcript,
                                     output_sha256=digest(strs))],
                focus_u=int(geometry[:, 0].sum()), focus_v=int(geometry[:, 1].sum()),
-               cartesian_opportunities=int(sum(u * v)), valid_focused_candidates=int(counts[:, 0].sum()),
+               cartesian_opportunities=cartesian, valid_focused_candidates=int(counts[:, 0].sum()),
                genuine_cubes=len(values) - len(hits), local_survivors=len(values), cube_checks=len(values),
                kernel_seconds=stats['kernel_ms'] / 1000, focus_enumeration_seconds=stats['window_ms'] / 1000,
                transfer_seconds=0.0, verification_seconds=verification_seconds,
@@ -206,14 +212,102 @@ def compute_lease(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, first: int
     return acc.finish(time.monotonic() - started)
 
 
+class _LeaseChunk:
+    """Host buffers for up to ``size`` leases of one ``pc_run_leases`` call, reused chunk after
+    chunk (the receipts copy everything they keep out of them)."""
+
+    def __init__(self, matcher: MaskedMatcher, size: int, width: int, output_records: int) -> None:
+        self.matcher, self.size, self.width, self.records = matcher, size, width, output_records
+        self.stride = len(matcher.filter_groups) + 3
+        ntmax = (LEASE_WIDTH + width - 1) // width
+        self.counts = [np.zeros(ntmax * self.stride, dtype=np.uint64) for _ in range(size)]
+        self.geometry = [np.zeros(2 * ntmax, dtype=np.uint64) for _ in range(size)]
+        self.out = [np.zeros(2 * output_records, dtype=np.uint64) for _ in range(size)]
+        self.n_out = np.zeros(size, dtype=np.uint64)
+        self.stats = (N.Stats * size)()
+        self.status = np.zeros(size, dtype=np.int32)
+        self.leases: list[tuple[int, int, float]] = []
+        self.future: Future | None = None
+
+    def submit(self, pool: ThreadPoolExecutor, af: GPUFocus, bf: GPUFocus, leases: list[tuple[int, int]]) -> None:
+        m, c = self.matcher, self.matcher.config
+        self.leases = [(first, end, time.monotonic()) for first, end in leases]
+        self.status[:] = 0
+        self.n_out[:] = 0
+        n = len(leases)
+        firsts = np.array([f for f, _ in leases], dtype=np.uint64)
+        ends = np.array([e for _, e in leases], dtype=np.uint64)
+        ptrs = lambda arrays: (ctypes.c_void_p * n)(*[x.ctypes.data for x in arrays[:n]])
+        args = (m.runtime.ctx, af.handle, bf.handle, m.filters.handle, ctypes.byref(m.tuning), n, firsts, ends,
+                self.width, c.lo & MASK, c.lo >> 64, c.hi & MASK, c.hi >> 64, ptrs(self.counts), ptrs(self.geometry),
+                ptrs(self.out), self.records, self.n_out, self.stats, self.status)
+
+        def run() -> int:
+            m.runtime.check()
+            return m.runtime.lib.pc_run_leases(*args)
+
+        self.future = pool.submit(run)
+
+    def wait(self, i: int) -> int:
+        """The return code of lease i, once its results are on the host."""
+        while self.status[i] == 0 and not self.future.done():
+            time.sleep(0.0002)
+        if self.status[i] == 0:                       # the call ended before lease i: its own failure
+            code = self.future.result()
+            self.matcher.runtime.call(code, 'lease list')
+            raise RuntimeError(f'lease list stopped before lease {i}')
+        return int(self.status[i]) - 1
+
+    def raw(self, i: int) -> dict[str, Any]:
+        first, end, _ = self.leases[i]
+        nt = (end - first + self.width - 1) // self.width
+        n = int(self.n_out[i])
+        m = self.matcher
+        m.last_stats = self.stats[i].as_dict()
+        return dict(counts=self.counts[i][:nt * self.stride].reshape(nt, self.stride),
+                    geometry=self.geometry[i][:2 * nt].reshape(nt, 2),
+                    per_tile=split_outputs(self.out[i][:2 * n].reshape(-1, 2), nt), stats=m.last_stats)
+
+    def finish(self) -> None:
+        self.future.result()
+
+
+class _LeaseCalls:
+    """The same protocol for a matcher with only ``run_lease``: one helper-thread call per lease."""
+
+    def __init__(self, matcher: Any, width: int) -> None:
+        self.matcher, self.width = matcher, width
+        self.leases: list[tuple[int, int, float]] = []
+        self.futures: list[Future] = []
+
+    def submit(self, pool: ThreadPoolExecutor, af: GPUFocus, bf: GPUFocus, leases: list[tuple[int, int]]) -> None:
+        self.leases = [(first, end, time.monotonic()) for first, end in leases]
+        self.futures = [pool.submit(self.matcher.run_lease, af, bf, first, end, self.width) for first, end in leases]
+
+    def wait(self, i: int) -> int:
+        self.futures[i].result()
+        return N.PC_OK
+
+    def raw(self, i: int) -> dict[str, Any]:
+        return self.futures[i].result()
+
+    def finish(self) -> None:
+        for future in self.futures:
+            future.result()
+
+
 def compute_leases(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, leases: Iterable[tuple[int, int]],
-                   heartbeat: Callable[[], None] = lambda: None) -> Iterator[dict[str, Any]]:
+                   heartbeat: Callable[[], None] = lambda: None, chunk: int = 4) -> Iterator[dict[str, Any]]:
     """Receipts of a sequence of leases, in order, each identical to ``compute_lease`` of it.
 
-    A worker that runs leases back to back overlaps them: the device call of lease k + 1 runs on a
-    helper thread (the library call releases the interpreter lock) while this thread builds and
-    re-verifies the receipt of lease k.  One device call is in flight at a time, so the library
-    context is never used by two threads at once.  Bounds are validated before a lease is issued."""
+    A worker that runs leases back to back overlaps them.  One helper thread runs the device work:
+    ``pc_run_leases`` over ``chunk`` leases at a time, with the next chunk queued behind it, so
+    consecutive leases follow each other on the device with no interpreter step between them.
+    This thread builds and re-verifies the receipt of each lease as soon as the library marks it
+    done.  Every device call goes through the one helper thread, so the library context is never
+    used by two threads at once.  A lease that fails in the list (an output buffer too small, say)
+    is rerun alone through ``MaskedMatcher.run_lease``, which applies the reference's overflow rule.
+    Bounds are validated before a lease is issued."""
     if not hasattr(matcher, 'run_lease'):
         for first, end in leases:
             yield compute_lease(matcher, af, bf, first, end, heartbeat)
@@ -221,21 +315,49 @@ def compute_leases(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, leases: I
     width = PROFILE['tile_width']
     pending = iter(leases)
 
-    def issue(pool: ThreadPoolExecutor) -> Optional[tuple[Future, int, int, float]]:
-        lease = next(pending, None)
-        if lease is None:
-            return None
-        first, end = lease
-        if not 0 <= first < end or end - first > LEASE_WIDTH:
-            raise ValueError('invalid optimized lease')
-        Tile(first, end).validate(matcher.config)
-        return pool.submit(matcher.run_lease, af, bf, first, end, width), first, end, time.monotonic()
+    def take() -> list[tuple[int, int]]:
+        out = []
+        for first, end in pending:
+            if not 0 <= first < end or end - first > LEASE_WIDTH:
+                raise ValueError('invalid optimized lease')
+            Tile(first, end).validate(matcher.config)
+            out.append((first, end))
+            if len(out) == chunk:
+                break
+        return out
 
     with ThreadPoolExecutor(max_workers=1) as pool:
-        current = issue(pool)
-        while current is not None:
-            future, first, end, started = current
-            raw = future.result()
-            heartbeat()
-            current = issue(pool)
-            yield lease_receipt(matcher, raw, first, end, started)
+        native = isinstance(matcher, MaskedMatcher)
+        slots = [_LeaseChunk(matcher, chunk, width, matcher.lease_output_records) if native else
+                 _LeaseCalls(matcher, width) for _ in range(2)]
+        running: deque = deque()
+        for slot in slots:
+            batch = take()
+            if batch:
+                slot.submit(pool, af, bf, batch)
+                running.append(slot)
+        while running:
+            slot = running[0]
+            for i, (first, end, started) in enumerate(slot.leases):
+                code = slot.wait(i)
+                if code == N.PC_OK:
+                    raw = slot.raw(i)
+                else:
+                    if code != N.PC_OVERFLOW:
+                        matcher.runtime.call(code, 'lease')
+                    rest = slot.leases[i:]
+                    slot.finish()
+                    raws = [pool.submit(matcher.run_lease, af, bf, f, e, width) for f, e, _ in rest]
+                    for (f, e, t0), fut in zip(rest, raws):
+                        result = fut.result()
+                        heartbeat()
+                        yield lease_receipt(matcher, result, f, e, t0)
+                    break
+                heartbeat()
+                yield lease_receipt(matcher, raw, first, end, started)
+            slot.finish()
+            running.popleft()
+            batch = take()
+            if batch:                                 # reuses the buffers of the chunk just consumed
+                slot.submit(pool, af, bf, batch)
+                running.append(slot)

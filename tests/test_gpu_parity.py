@@ -183,6 +183,12 @@ def test_overlapped_leases_equal_one_by_one(runtime, p619, focuses619):
     want = [strip(compute_lease(matcher, fa, fb, first, end)) for first, end in leases]
     assert got == want
     assert got[0]['subtile_scopes'][0]['transcript_sha256'] == gold['transcript_sha256']
+    # two chunks through the same buffers, and a lease whose outputs overflow the list's buffer
+    # (rerun alone under the reference's overflow rule)
+    assert [strip(r) for r in compute_leases(matcher, fa, fb, leases[::-1] + leases, chunk=2)] == want[::-1] + want
+    small = MaskedMatcher(runtime, p619)
+    small.lease_output_records = 16                  # the golden lease emits 82 values
+    assert [strip(r) for r in compute_leases(small, fa, fb, leases, chunk=2)] == want
     with pytest.raises(ValueError):
         list(compute_leases(matcher, fa, fb, [(10, 10)]))
 
