@@ -118,7 +118,8 @@ def max_over_ranks(dist, value: float, local: int) -> float:
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f'cuda:{local}')
+    device = 'cpu' if dist.get_backend() == 'gloo' else f'cuda:{local}'
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

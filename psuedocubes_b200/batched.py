@@ -81,6 +81,14 @@ class BatchedEngine:
         self._families: dict[tuple[int, int, int], Filters] = {}
         self._pairs: dict[tuple[int, int], tuple[GPUFocus, GPUFocus]] = {}
         self._configs: dict[tuple[int, ...], Config] = {}
+        self._records = np.empty(0, dtype=np.uint64)
+
+    def record_buffer(self, records: int) -> np.ndarray:
+        """A host buffer for ``records`` output records, kept and reused by every batch (results are
+        copied out of it), so no step allocates and faults in a fresh output-sized array."""
+        if self._records.size < 2 * records:
+            self._records = np.empty(2 * records, dtype=np.uint64)
+        return self._records
 
     def focus(self, focus: Any) -> GPUFocus:
         key = (focus.modulus, focus.rings)
@@ -200,14 +208,14 @@ class WindowBatch:
 
     def raw(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
         rt = self.runtime
-        counts = np.zeros(max(1, self.ntiles * self.stride), dtype=np.uint64)
-        geometry = np.zeros(max(2, 2 * self.ntiles), dtype=np.uint64)
-        records = np.zeros(2 * max(1, self.output_cap), dtype=np.uint64)
+        counts = np.empty(max(1, self.ntiles * self.stride), dtype=np.uint64)     # every entry is written
+        geometry = np.empty(max(2, 2 * self.ntiles), dtype=np.uint64)
+        records = self.engine.record_buffer(max(1, self.output_cap))
         n_out = ctypes.c_uint64()
         rt.call(rt.lib.pc_multi_results(rt.ctx, self.handle, counts, geometry, records, self.output_cap,
                                         ctypes.byref(n_out)))
         return (counts[:self.ntiles * self.stride].reshape(self.ntiles, self.stride),
-                geometry[:2 * self.ntiles].reshape(self.ntiles, 2), records[:2 * n_out.value].reshape(-1, 2))
+                geometry[:2 * self.ntiles].reshape(self.ntiles, 2), records[:2 * n_out.value].reshape(-1, 2).copy())
 
     def positions(self) -> int:
         """Focused candidate positions of the last run (all windows)."""
