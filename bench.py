@@ -262,6 +262,16 @@ def run_ours(args) -> None:
                              d2h_bytes_per_step=int(d2h), api='psuedocubes_b200.optimized.compute_leases'),
                     gpu_launches=launches, clocks=clock, tuning=effective,
                     kernel_ms_per_step=kernel_ms / args.steps, stage_ms_per_step=stage_ms)
+        if kernel_ms and effective.get('bitset_filters'):
+            # the resource k_match actually saturates: shared-memory bandwidth of the bitset tier,
+            # which reads one 16-byte row unit per bitset filter per 128 positions
+            smem_bytes = effective['bitset_filters'] * 16 / 128 * positions
+            smem_peak = runtime.sm_count * 128 * sm_mhz * 1e6 / 1e12          # TB/s, 128 B per clock per SM
+            smem_achieved = smem_bytes / (kernel_ms / 1000) / 1e12
+            line['roofline']['shared_memory'] = dict(
+                bound='smem', achieved=smem_achieved, peak=smem_peak, unit='TB/s', frac=smem_achieved / smem_peak,
+                bytes_per_position=effective['bitset_filters'] * 16 / 128,
+                basis='bitset-tier row reads only (survivor recompute, row build and cheap tier add to them)')
         if world == 1 and not args.no_cpu:
             line['cpu_baseline'] = {k: v for k, v in cpu_sample(1, args.warmup, batches=8).items()
                                     if k in ('value', 'unit', 'cores', 'kind', 'sample')}
