@@ -258,3 +258,27 @@ def test_coordinates_upload_roundtrip(runtime):
     assert np.array_equal(arr[1:3].get(), data[1:3])
     assert arr.searchsorted([0, 5, 6, 2**64 - 1]).tolist() == [0, 1, 2, 4]
     assert arr[1:3].searchsorted([0, 5, 6, 2**64 - 1]).tolist() == [0, 0, 1, 2]
+
+
+@pytest.mark.parametrize('index', [0, 3])
+def test_bench_lease_batches_match_oracle(runtime, p619, focuses619, oracle, oracle619, index):
+    """The leases bench.py times (its warm-up lease 0 and first timed lease 3): the first, a middle
+    and the last batch of each, subtile by subtile, against the oracle."""
+    import bench
+    fa, fb = focuses619
+    g, ofa, ofb = oracle619
+    first, end = bench.lease_bounds(index)
+    raw = MaskedMatcher(runtime, p619).run_lease(fa, fb, first, end, 100_000_000)
+    ng = len(p619.filter_groups())
+    for b in (0, 131, 255):
+        start = first + b * BATCH_WIDTH
+        want = oracle.batch(g, ofa, ofb, start, start + BATCH_WIDTH)
+        for k, scope in enumerate(want['subtile_scopes']):
+            t = 64 * b + k
+            row = raw['counts'][t]
+            assert int(row[0]) == scope['valid_focused_candidates'], (b, k)
+            assert [int(n) for n in row[1:ng + 1]] == scope['group_survivors'], (b, k)
+            assert int(row[ng + 1]) == scope['local_survivors'] and int(row[ng + 2]) == 0
+            assert oracle.digest([str(n) for n in raw['per_tile'][t]]) == scope['output_sha256']
+        geo = raw['geometry'][64 * b:64 * b + 64]
+        assert int(geo[:, 0].sum()) == want['focus_u'] and int(geo[:, 1].sum()) == want['focus_v']
