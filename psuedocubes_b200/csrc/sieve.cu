@@ -436,10 +436,10 @@ __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bit
 // The unit loop of one (v row, block) piece: AND of the NB rows per 16-byte unit, range masks
 // unless the row covers the whole block (FULL), the group-1 popcount (first four filters) and,
 // when group 2 ends at the last bitset filter (C2), the group-2 popcount.  Returns the mask of
-// units that keep a bit after every bitset filter.
+// units that keep a bit after every bitset filter; save receives the bits of the first of them.
 template <int NB, int U, bool FULL, bool C2>
 __device__ __forceinline__ uint32_t piece_units(const uint4 *__restrict__ rows, const uint32_t (&ro)[NB],
-                                                uint32_t lane, int32_t s, int32_t e, uint32_t (&c)[3]) {
+                                                uint32_t lane, int32_t s, int32_t e, uint32_t (&c)[3], uint4 &save) {
     uint32_t pend = 0;
 #pragma unroll
     for (uint32_t p = 0; p < U; ++p) {
@@ -465,7 +465,9 @@ __device__ __forceinline__ uint32_t piece_units(const uint4 *__restrict__ rows, 
         }
         c[0] += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
         if (C2) c[1] += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
-        pend |= (uint32_t)((acc.x | acc.y | acc.z | acc.w) != 0) << p;
+        const bool live = (acc.x | acc.y | acc.z | acc.w) != 0;
+        if (live && !pend) save = acc;                // the first marked unit is not read again
+        pend |= (uint32_t)live << p;
     }
     return pend;
 }
@@ -478,9 +480,10 @@ __device__ __forceinline__ void copy_words(void *dst, const void *src, uint32_t 
 // (lane + p) mod (K/4), so at every step the 32 lanes of a warp hit each 16-byte bank group
 // exactly 32/(K/4) times whatever rows they read.  Group counters of groups 1..3 live in
 // registers (c[0..2]) and are reduced per subtile when a lane's subtile changes.  The unit loop
-// only marks the units that keep a bit after every bitset filter; once the piece is done, the
-// lanes recompute their marked units and queue the bits, so the warp votes and diverges once per
-// piece instead of after every unit.
+// only marks the units that keep a bit after every bitset filter (and keeps the bits of the
+// first one in registers); once the piece is done, the lanes take their marked units (the first
+// from registers, any further one re-read) and queue the bits, so the warp votes and diverges
+// once per piece instead of after every unit.
 template <int NB, int K, int NT>
 __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     using G = Geo<K>;
@@ -668,16 +671,25 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             // warp-uniform FULL and block-uniform C2 select the loop body, so the range masks and the
             // group-2 popcounts are not issued (as predicated code) where they cannot apply
             uint32_t pend;                                // units of this piece with survivors
+            uint4 save;                                   // bits of its first one
             if (full)
-                pend = c2_live ? piece_units<NB, U, true, true>(rows, ro, lane, s, e, c)
-                               : piece_units<NB, U, true, false>(rows, ro, lane, s, e, c);
+                pend = c2_live ? piece_units<NB, U, true, true>(rows, ro, lane, s, e, c, save)
+                               : piece_units<NB, U, true, false>(rows, ro, lane, s, e, c, save);
             else
-                pend = c2_live ? piece_units<NB, U, false, true>(rows, ro, lane, s, e, c)
-                               : piece_units<NB, U, false, false>(rows, ro, lane, s, e, c);
+                pend = c2_live ? piece_units<NB, U, false, true>(rows, ro, lane, s, e, c, save)
+                               : piece_units<NB, U, false, false>(rows, ro, lane, s, e, c, save);
+            bool saved = pend != 0;                       // the next marked unit is the saved one
             while (__any_sync(0xffffffffu, pend != 0)) {      // recompute a marked unit, queue its bits
                 uint4 acc = make_uint4(0, 0, 0, 0);
                 uint32_t u = 0;
-                if (pend) {
+                const bool again = pend != 0 && !saved;
+                if (saved) {
+                    const uint32_t p = __ffs(pend) - 1;
+                    pend &= pend - 1;
+                    u = (lane + p) & (U - 1);
+                    acc = save;
+                    saved = false;
+                } else if (again) {
                     const uint32_t p = __ffs(pend) - 1;
                     pend &= pend - 1;
                     u = (lane + p) & (U - 1);
