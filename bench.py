@@ -155,7 +155,7 @@ def run_reference(args) -> None:
         return
     for _ in range(max(0, min(args.warmup, 1))):
         cpu_sample(1, 0, batches=4)
-    sample = cpu_sample(args.steps, args.warmup, batches=8)
+    sample = cpu_sample(args.steps, args.warmup, batches=32)
     line = dict(metric=METRIC, value=sample['value'], unit=UNIT, n_gpus=args.gpus, steps=args.steps,
                 warmup=args.warmup, ms_per_step=1000 * sample['seconds'] / max(1, args.steps),
                 higher_is_better=True, scaling='weak', vs_baseline=None, dtype='u64', data='synthetic',
@@ -273,7 +273,7 @@ def run_ours(args) -> None:
                 bytes_per_position=effective['bitset_filters'] * 16 / 128,
                 basis='bitset-tier row reads only (survivor recompute, row build and cheap tier add to them)')
         if world == 1 and not args.no_cpu:
-            line['cpu_baseline'] = {k: v for k, v in cpu_sample(1, args.warmup, batches=8).items()
+            line['cpu_baseline'] = {k: v for k, v in cpu_sample(1, args.warmup, batches=64).items()
                                     if k in ('value', 'unit', 'cores', 'kind', 'sample')}
         print(json.dumps(line), flush=True)
     del af, bf, matcher
