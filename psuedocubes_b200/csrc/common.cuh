@@ -204,6 +204,7 @@ struct WinBatch {
     uint64_t units = 0;
     void *d_desc = nullptr, *d_foci = nullptr;
     uint64_t *d_cnt = nullptr, *d_off = nullptr, *d_ws = nullptr, *d_tot = nullptr, *d_base = nullptr;
+    uint32_t *d_bits = nullptr;      // the count pass's unit words for the emit pass (null: recompute)
     std::vector<uint64_t> total, base;
     uint64_t out_len = 0;
 };

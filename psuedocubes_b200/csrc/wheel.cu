@@ -37,6 +37,7 @@ namespace {
 constexpr int WT = 256;          // threads per CTA of the window kernels
 constexpr int SIEVE_WORDS = 64;  // sieve words per thread
 constexpr int WIN_WORDS = 32;    // wheel words per window unit
+constexpr uint64_t WIN_WORDS_BUDGET = UINT64_C(512) << 20;   // kept count-pass words, bytes
 
 // Periodic bit patterns of the S rings, replicated so any 32-bit window at offset < q is one
 // funnel shift of two consecutive words.
@@ -159,12 +160,13 @@ constexpr int WIN_UNITS_PER_WARP = 16;
 // the window of its first unit by a binary search over the windows' first units and steps to the
 // next window when its units cross into it.  The row addresses of a period are computed once and
 // reused while its units stay in that period (a period spans hundreds of units), and the rows of a
-// unit are loaded together before they are combined.  Count pass: per-unit totals.  Emit pass: the lane's
-// exclusive prefix inside the warp, plus the unit's offset inside its window, plus the window's
-// base gives ascending output slots.
+// unit are loaded together before they are combined.  Count pass: per-unit totals, and (words
+// not null) each unit's 32 words kept for the emit pass, which then reads them instead of the
+// rows.  Emit pass: the lane's exclusive prefix inside the warp, plus the unit's offset inside
+// its window, plus the window's base gives ascending output slots.
 __global__ void k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, const FocusDev *__restrict__ foci,
                           uint64_t units, uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
-                          const uint64_t *__restrict__ bases, uint64_t *__restrict__ out) {
+                          const uint64_t *__restrict__ bases, uint64_t *__restrict__ out, uint32_t *__restrict__ words) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t u0 = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * WIN_UNITS_PER_WARP;
     if (u0 >= units) return;                            // warp-uniform
@@ -192,32 +194,37 @@ __global__ void k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, cons
         unit_of(p, f.words1, gu - ubase, K, wa, wb);
         const uint64_t w = wa + lane;
         uint32_t bits = 0;
-        if (K != row_K || lo != row_win) {             // warp-uniform
-            row_K = K;
-            row_win = lo;
+        if (offsets && words) {                         // emit pass: the count pass kept the words
+            bits = words[gu * 32 + lane];
+        } else {
+            if (K != row_K || lo != row_win) {             // warp-uniform
+                row_K = K;
+                row_win = lo;
 #pragma unroll
-            for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) {
-                row[t] = f.rows;                        // rows past nT: a valid address, never read
-                if (t < f.nT) {
-                    const uint32_t s = fastmod32(mod64(K, f.tmq[t]) * f.t_m1mod[t], f.tmq[t].c, f.tq[t]);   // < q^2 < 2^32
-                    row[t] += (uint64_t)(f.t_row0[t] + s) * f.words1;
+                for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) {
+                    row[t] = f.rows;                        // rows past nT: a valid address, never read
+                    if (t < f.nT) {
+                        const uint32_t s = fastmod32(mod64(K, f.tmq[t]) * f.t_m1mod[t], f.tmq[t].c, f.tq[t]);   // < q^2 < 2^32
+                        row[t] += (uint64_t)(f.t_row0[t] + s) * f.words1;
+                    }
                 }
             }
-        }
-        if (w < wb) {
-            bits = 0xffffffffu;
-            if (f.nT) {                                 // all row loads in flight before the first use
-                uint32_t r[PC_MAX_WHEEL_T];
+            if (w < wb) {
+                bits = 0xffffffffu;
+                if (f.nT) {                                 // all row loads in flight before the first use
+                    uint32_t r[PC_MAX_WHEEL_T];
 #pragma unroll
-                for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) r[t] = t < f.nT ? __ldg(row[t] + w) : 0xffffffffu;
+                    for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) r[t] = t < f.nT ? __ldg(row[t] + w) : 0xffffffffu;
 #pragma unroll
-                for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) bits &= r[t];
+                    for (uint32_t t = 0; t < PC_MAX_WHEEL_T; ++t) bits &= r[t];
+                }
+                const uint64_t jmin = K == p.K0 ? p.j_lo : 0;
+                const uint64_t jmax = K == p.K1 ? p.j_hi : f.count1;
+                const uint64_t j0 = w * 32;
+                if (j0 < jmin) bits &= ~low_bits((uint32_t)(jmin - j0 < 32 ? jmin - j0 : 32));
+                if (j0 + 32 > jmax) bits &= jmax > j0 ? low_bits((uint32_t)(jmax - j0)) : 0u;
             }
-            const uint64_t jmin = K == p.K0 ? p.j_lo : 0;
-            const uint64_t jmax = K == p.K1 ? p.j_hi : f.count1;
-            const uint64_t j0 = w * 32;
-            if (j0 < jmin) bits &= ~low_bits((uint32_t)(jmin - j0 < 32 ? jmin - j0 : 32));
-            if (j0 + 32 > jmax) bits &= jmax > j0 ? low_bits((uint32_t)(jmax - j0)) : 0u;
+            if (words) words[gu * 32 + lane] = bits;
         }
         const uint32_t n = __popc(bits);
         if (!offsets) {
@@ -527,7 +534,7 @@ int winbatch_count(pc_ctx *ctx, const WinBatch &wb) {
         const uint64_t warps = (wb.units + WIN_UNITS_PER_WARP - 1) / WIN_UNITS_PER_WARP;
         const unsigned grid = (unsigned)((warps * 32 + WT - 1) / WT);
         k_windows<<<grid, WT, 0, ctx->stream>>>((const WinDesc *)wb.d_desc, wb.n, (const FocusDev *)wb.d_foci, wb.units,
-                                                wb.d_cnt, nullptr, nullptr, nullptr);
+                                                wb.d_cnt, nullptr, nullptr, nullptr, wb.d_bits);
         PC_LAUNCHED(ctx, "window count");
     }
     return pc_exclusive_scan_ws(ctx, wb.d_cnt, wb.d_off, wb.units, wb.d_off + wb.units, wb.d_ws);
@@ -540,7 +547,7 @@ int winbatch_emit(pc_ctx *ctx, const WinBatch &wb, uint64_t *out) {
         const uint64_t warps = (wb.units + WIN_UNITS_PER_WARP - 1) / WIN_UNITS_PER_WARP;
         const unsigned grid = (unsigned)((warps * 32 + WT - 1) / WT);
         k_windows<<<grid, WT, 0, ctx->stream>>>((const WinDesc *)wb.d_desc, wb.n, (const FocusDev *)wb.d_foci, wb.units,
-                                                nullptr, wb.d_off, wb.d_base, out);
+                                                nullptr, wb.d_off, wb.d_base, out, wb.d_bits);
         PC_LAUNCHED(ctx, "window emit");
     }
     return PC_OK;
@@ -577,6 +584,9 @@ int winbatch_plan(pc_ctx *ctx, Scratch &hold, const pc_focus *const *focus, cons
     if (!rc) rc = hold.get(&wb.d_ws, pc_scan_workspace(wb.units));
     if (!rc) rc = hold.get(&wb.d_tot, n);
     if (!rc) rc = hold.get(&wb.d_base, n);
+    // keep the count pass's unit words for the emit pass when they fit WIN_WORDS_BUDGET bytes
+    if (!rc && wb.units * WIN_WORDS * 4 <= WIN_WORDS_BUDGET && ctx->in_use + wb.units * WIN_WORDS * 4 <= ctx->cap / 2)
+        rc = hold.get(&wb.d_bits, wb.units * WIN_WORDS);
     if (rc) return rc;
     wb.d_desc = d_desc;
     wb.d_foci = d_foci;
