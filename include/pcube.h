@@ -43,6 +43,12 @@ int pc_init(int device, uint64_t mem_cap, double fraction, pc_ctx **out);
 int pc_free(pc_ctx *ctx);
 int pc_mem_info(const pc_ctx *ctx, uint64_t *in_use, uint64_t *peak, uint64_t *cap);
 int pc_device_info(const pc_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor, char *name, int name_len);
+
+/* Page-locked host memory for result buffers (counts, geometry, outputs): device-to-host copies
+ * into it run at full link speed instead of through the driver's staging.  PC_NOMEM when it cannot
+ * be had; free with pc_host_free (which waits for the device). */
+int pc_host_alloc(uint64_t bytes, void **out);
+int pc_host_free(void *p);
 int pc_sync(pc_ctx *ctx);
 /* Device timestamps on the context's stream (slot 0..7) and the milliseconds between two. */
 int pc_mark(pc_ctx *ctx, int slot);

@@ -9,6 +9,7 @@ from __future__ import annotations
 import ctypes
 import hashlib
 import time
+import weakref
 from functools import lru_cache
 from pathlib import Path
 from typing import Any
@@ -21,7 +22,7 @@ LIB_PATH = LIB_DIR / 'libpcube.so'
 PC_OK, PC_OVERFLOW, PC_INVALID, PC_ARITHMETIC, PC_TIMEOUT, PC_NOMEM, PC_CUDA = range(7)
 
 #: Every symbol include/pcube.h declares.
-SYMBOLS = ('pc_version', 'pc_device_count', 'pc_last_error', 'pc_init', 'pc_free', 'pc_mem_info',
+SYMBOLS = ('pc_version', 'pc_device_count', 'pc_last_error', 'pc_init', 'pc_free', 'pc_mem_info', 'pc_host_alloc', 'pc_host_free',
            'pc_device_info', 'pc_sync', 'pc_mark', 'pc_elapsed', 'pc_buf_upload', 'pc_buf_download', 'pc_buf_size', 'pc_buf_free',
            'pc_buf_searchsorted', 'pc_focus_create', 'pc_focus_free', 'pc_focus_info', 'pc_focus_window',
            'pc_filters_create', 'pc_filters_free', 'pc_run_batch', 'pc_run_lease', 'pc_run_leases', 'pc_multi_create',
@@ -117,6 +118,8 @@ def lib() -> ctypes.CDLL:
     so.pc_run_leases.argtypes = [_P, _P, _P, _P, ctypes.POINTER(Tuning), _U32, _U64P, _U64P, _U64, _U64, _U64, _U64, _U64,
                                  pp, pp, pp, _U64, _U64P, ctypes.POINTER(Stats),
                                  np.ctypeslib.ndpointer(dtype=np.int32, flags='C_CONTIGUOUS')]
+    so.pc_host_alloc.argtypes = [_U64, ctypes.POINTER(_P)]
+    so.pc_host_free.argtypes = [_P]
     so.pc_cube_roots.argtypes = [_P, _U64, _U64, _U32, ctypes.c_void_p, _U64, ctypes.POINTER(_U64),
                                  ctypes.POINTER(ctypes.c_double)]
     so.pc_selftest_wide.argtypes = [_P, _U64P, _U64P, _U64]
@@ -153,6 +156,21 @@ def raise_for(code: int, ctx: Any = None, what: str = '') -> None:
     if code == PC_NOMEM:
         raise MemoryError(message)
     raise RuntimeError(f'CUDA failure in libpcube: {message}')
+
+
+def pinned(count: int, dtype: Any = np.uint64) -> np.ndarray:
+    """A zeroed numpy array in page-locked host memory (pc_host_alloc), freed with the array; the
+    library copies results into such buffers at full link speed."""
+    dtype = np.dtype(dtype)
+    nbytes = max(1, int(count)) * dtype.itemsize
+    ptr = _P()
+    so = lib()
+    raise_for(so.pc_host_alloc(nbytes, ctypes.byref(ptr)), None, 'page-locked host buffer')
+    raw = (ctypes.c_uint8 * nbytes).from_address(ptr.value)
+    array = np.frombuffer(raw, dtype=np.uint8).view(dtype)[:max(0, int(count))]
+    array[:] = 0
+    weakref.finalize(raw, so.pc_host_free, ptr.value)
+    return array
 
 
 def device_count() -> int:

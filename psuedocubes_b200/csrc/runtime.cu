@@ -90,6 +90,25 @@ extern "C" int pc_init(int device, uint64_t mem_cap, double fraction, pc_ctx **o
     return PC_OK;
 }
 
+extern "C" int pc_host_alloc(uint64_t bytes, void **out) {
+    if (!out) return PC_INVALID;
+    *out = nullptr;
+    if (cudaHostAlloc(out, std::max<uint64_t>(bytes, 16), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return PC_NOMEM;
+    }
+    return PC_OK;
+}
+
+extern "C" int pc_host_free(void *p) {
+    if (p && cudaFreeHost(p) != cudaSuccess) {
+        cudaGetLastError();
+        return PC_CUDA;
+    }
+    return PC_OK;
+}
+
 extern "C" int pc_free(pc_ctx *ctx) {
     if (!ctx) return PC_OK;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);

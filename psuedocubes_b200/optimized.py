@@ -220,8 +220,9 @@ class _LeaseChunk:
         self.matcher, self.size, self.width, self.records = matcher, size, width, output_records
         self.stride = len(matcher.filter_groups) + 3
         ntmax = (LEASE_WIDTH + width - 1) // width
-        self.counts = [np.zeros(ntmax * self.stride, dtype=np.uint64) for _ in range(size)]
-        self.geometry = [np.zeros(2 * ntmax, dtype=np.uint64) for _ in range(size)]
+        # page-locked: the library's device-to-host copies at the end of each lease run at full speed
+        self.counts = [N.pinned(ntmax * self.stride) for _ in range(size)]
+        self.geometry = [N.pinned(2 * ntmax) for _ in range(size)]
         self.out = [np.zeros(2 * output_records, dtype=np.uint64) for _ in range(size)]
         self.n_out = np.zeros(size, dtype=np.uint64)
         self.stats = (N.Stats * size)()
@@ -327,9 +328,16 @@ def compute_leases(matcher: MaskedMatcher, af: GPUFocus, bf: GPUFocus, leases: I
         return out
 
     with ThreadPoolExecutor(max_workers=1) as pool:
-        native = isinstance(matcher, MaskedMatcher)
-        slots = [_LeaseChunk(matcher, chunk, width, matcher.lease_output_records) if native else
-                 _LeaseCalls(matcher, width) for _ in range(2)]
+        if isinstance(matcher, MaskedMatcher):
+            # page-locked buffers are slow to allocate: the matcher keeps its two chunks for later calls
+            key = (chunk, width, matcher.lease_output_records)
+            kept = getattr(matcher, '_lease_chunks', None)
+            if kept is None or kept[0] != key:
+                kept = (key, [_LeaseChunk(matcher, chunk, width, matcher.lease_output_records) for _ in range(2)])
+                matcher._lease_chunks = kept
+            slots = kept[1]
+        else:
+            slots = [_LeaseCalls(matcher, width) for _ in range(2)]
         running: deque = deque()
         for slot in slots:
             batch = take()
