@@ -163,8 +163,10 @@ constexpr int WIN_UNITS_PER_WARP = 16;
 // unit are loaded together before they are combined.  Count pass: per-unit totals, and (words
 // not null) each unit's 32 words kept for the emit pass, which then reads them instead of the
 // rows.  Emit pass: the lane's exclusive prefix inside the warp, plus the unit's offset inside
-// its window, plus the window's base gives ascending output slots.
-__global__ void k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, const FocusDev *__restrict__ foci,
+// its window, plus the window's base gives ascending output slots.  Both passes wait on L2 (row
+// words, wheel entries), so the kernel is held to 32 registers for 64 resident warps per SM; the
+// few spills sit on the once-per-period row-address path.
+__global__ void __launch_bounds__(WT, 8) k_windows(const WinDesc *__restrict__ desc, uint32_t ndesc, const FocusDev *__restrict__ foci,
                           uint64_t units, uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
                           const uint64_t *__restrict__ bases, uint64_t *__restrict__ out, uint32_t *__restrict__ words) {
     const uint32_t lane = threadIdx.x & 31;
