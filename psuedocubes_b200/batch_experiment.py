@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes
 import time
+from collections.abc import Sequence
 from dataclasses import dataclass
 from typing import Any
 
@@ -20,7 +21,7 @@ from .accounting import EMPTY_DIGEST, digest, scope_list
 from .focus import Config, Tile
 from .gpu import MASK, DeviceArray, Filters, GPUFocus, Matcher, Runtime, launch_plan
 from .predicate import is_perfect_cube, local3
-from .verify import verify
+from .verify import MATERIALISE_MAX, VECTOR_MIN, verify, verify_many
 
 
 @dataclass
@@ -102,10 +103,22 @@ def split_outputs(records: np.ndarray, ntiles: int) -> list[list[int]]:
     return per
 
 
-def verify_values(config: Config, values: list[int]) -> list[dict[str, Any]]:
-    """Host re-check of every emitted value (pseudocube/batch_experiment.py:138-144)."""
+def verify_values(config: Config, values: list[int]) -> Sequence[dict[str, Any]]:
+    """Host re-check of every emitted value (pseudocube/batch_experiment.py:138-144).  Many values
+    are checked column-wise on all host cores (verify_many: the same predicates, the same rows)."""
     if len(values) != len(set(values)):
         raise ArithmeticError('duplicate canonical output')
+    if len(values) >= VECTOR_MIN and config.hi < 1 << 96:
+        if any(not config.lo < n <= config.hi for n in (min(values), max(values))):
+            raise ArithmeticError('GPU/CPU disagreement')
+        lo = np.fromiter((n & MASK for n in values), dtype=np.uint64, count=len(values))
+        hi = np.fromiter((n >> 64 for n in values), dtype=np.uint64, count=len(values))
+        ok, _, hits = verify_many(lo, hi, config.p)
+        if not ok.all():
+            raise ArithmeticError('GPU/CPU disagreement')
+        if not hits.all_valid:
+            raise ArithmeticError('independent witness verification failed')
+        return list(hits) if len(hits) <= MATERIALISE_MAX else hits
     if any(not config.lo < n <= config.hi or not local3(n, config.p) for n in values):
         raise ArithmeticError('GPU/CPU disagreement')
     hits = [verify(n, config.p) for n in values if not is_perfect_cube(n)]

@@ -39,7 +39,7 @@ from .cubes import genuine_cube_count
 from .focus import Config, Tile
 from .gpu import Matcher, Runtime
 from .tables import allowed
-from .verify import verify
+from .verify import MATERIALISE_MAX, VECTOR_MIN, cube_limbs, icbrt_many, verify, verify_many
 
 A_RINGS = (2, 7, 13, 31, 43, 73, 79, 127, 139, 157, 181)   # the rings of A619, ascending
 B_RINGS = (9, 19, 37, 61, 67, 97, 103, 109, 151, 163)      # the rings of B619, ascending
@@ -184,21 +184,9 @@ def _residues(lo: np.ndarray, hi: np.ndarray, q: int) -> np.ndarray:
 
 
 def _cube_mask(lo: np.ndarray, hi: np.ndarray) -> np.ndarray:
-    """x is a perfect cube, exactly: a = round(cbrt(x)) from a double (within 1 of the root for
-    x < 2^96), then a^3 compared in 128-bit limbs for a - 1, a, a + 1."""
-    xf = hi.astype(np.float64) * 18446744073709551616.0 + lo.astype(np.float64)
-    a0 = np.rint(np.cbrt(xf)).astype(np.int64)
-    found = np.zeros(len(lo), dtype=bool)
-    for d in (-1, 0, 1):
-        a = np.maximum(a0 + d, 0).astype(np.uint64)                   # a < 2^32
-        sq = a * a                                                    # < 2^64
-        h, l = sq >> np.uint64(32), sq & np.uint64(0xFFFFFFFF)
-        ha, la = h * a, l * a                                         # a^3 = ha 2^32 + la
-        low = (ha << np.uint64(32)) + la
-        carry = (low < la).astype(np.uint64)
-        high = (ha >> np.uint64(32)) + carry
-        found |= (low == lo) & (high == hi)
-    return found
+    """x is a perfect cube, exactly: the floor cube root (icbrt_many) cubed in 128-bit limbs."""
+    h, l = cube_limbs(icbrt_many(lo, hi))
+    return (h == hi) & (l == lo)
 
 
 def verify_outputs(records: np.ndarray, lo: int, hi: int, p: int) -> tuple[list[int], int, list[dict[str, Any]]]:
@@ -227,8 +215,13 @@ def verify_outputs(records: np.ndarray, lo: int, hi: int, p: int) -> tuple[list[
         ok &= table[_residues(xl, xh, q).astype(np.int64)]
     if not ok.all():
         raise ArithmeticError('GPU/CPU disagreement: local test failed')
-    cubes = _cube_mask(xl, xh)
     values = [h << 64 | l for h, l in zip(xh.tolist(), xl.tolist())]
+    if len(values) >= VECTOR_MIN:                        # the standalone verifier, column-wise
+        _, cubes, witnesses = verify_many(xl, xh, p)
+        if not witnesses.all_valid:
+            raise ArithmeticError('independent witness verification failed')
+        return values, int(cubes.sum()), list(witnesses) if len(witnesses) <= MATERIALISE_MAX else witnesses
+    cubes = _cube_mask(xl, xh)
     hits = [verify(n, p) for n, c in zip(values, cubes.tolist()) if not c]
     if any(not h['valid_pseudocube'] for h in hits):
         raise ArithmeticError('independent witness verification failed')

@@ -2,8 +2,8 @@
 of the batched engine: every focused position, the three group populations and the complete
 survivor list (65,848,989 values, 2,721 of them genuine cubes) against the CPU restatement's
 figures for this split.  The survivor list is checked by count, by the sha256 of its ascending
-decimal strings (the reference's digest encoding), by its genuine-cube count and by the vectorised
-local test."""
+decimal strings (the reference's digest encoding), by its genuine-cube count, by the vectorised
+local test and by the standalone witness verifier run column-wise over all 65.8M values."""
 from __future__ import annotations
 
 import hashlib
@@ -15,6 +15,7 @@ from psuedocubes_b200.batched import BatchedEngine, Window
 from psuedocubes_b200.served import _cube_mask, _residues
 from psuedocubes_b200.predicate import primes_upto
 from psuedocubes_b200.tables import allowed
+from psuedocubes_b200.verify import verify, verify_many
 
 pytestmark = pytest.mark.gpu
 
@@ -47,6 +48,13 @@ def test_p67_whole_domain(runtime):
             ok &= table[_residues(lo, zero, q).astype(np.int64)]
     assert ok.all()
     assert int(_cube_mask(lo, zero).sum()) == EXPECT['cubes']
+    # the standalone witness verifier over every survivor, column-wise on the host cores
+    local, cube, rows = verify_many(lo, zero, 67)
+    assert local.all() and rows.all_valid and int(cube.sum()) == EXPECT['cubes']
+    assert len(rows) == EXPECT['values'] - EXPECT['cubes']
+    noncube = lo[~cube]
+    for i in range(0, len(rows), len(rows) // 97):
+        assert rows[i] == verify(int(noncube[i]), 67)
     h = hashlib.sha256(b'[')
     for k in range(0, len(lo), 1 << 20):
         chunk = ','.join('"%d"' % n for n in lo[k:k + (1 << 20)].tolist())
