@@ -239,10 +239,9 @@ class WindowBatch:
                 per_tile[int(tile[k]) - t0].append(int(lo[k]) | (int(hi[k]) << 64))
             for values in per_tile:
                 values.sort()
-            ranges = []
+            ranges = []                                   # subtile v ranges (the u bounds are not read)
             for v in range(w.first, w.end, self.widths[i]):
-                stop = min(v + self.widths[i], w.end)
-                ranges.append((v, stop, c.u_interval(v)[0], c.u_interval(stop - 1)[1]))
+                ranges.append((v, min(v + self.widths[i], w.end), 0, 0))
             geo = [(int(a), int(b)) for a, b in geometry[t0:t1]]
             row = batch_result(c, ranges, pops, per_tile, geo, fam.filter_groups, 1 << 62)
             row.update(p=w.p, first=str(w.first), end=str(w.end), focus_u=int(self.sizes[2 * i]),
