@@ -193,6 +193,23 @@ def test_overlapped_leases_equal_one_by_one(runtime, p619, focuses619):
         list(compute_leases(matcher, fa, fb, [(10, 10)]))
 
 
+def test_overlapped_leases_stopped_early(runtime, p619, focuses619):
+    """A consumer that stops after two receipts: the leases already issued finish on the helper
+    thread before the generator returns, and the context is free for the next call."""
+    fa, fb = focuses619
+    matcher = MaskedMatcher(runtime, p619)
+    leases = [(12345 + k * BATCH_WIDTH, 12345 + (k + 1) * BATCH_WIDTH) for k in range(6)]
+    beats = []
+    gen = compute_leases(matcher, fa, fb, leases, heartbeat=lambda: beats.append(1), chunk=2)
+    got = [next(gen), next(gen)]
+    gen.close()
+    assert len(beats) == 2
+    strip = lambda r: {k: v for k, v in r.items() if not k.endswith('_seconds')}
+    assert [strip(r) for r in got] == [strip(compute_lease(matcher, fa, fb, f, e)) for f, e in leases[:2]]
+    again = compute_lease(matcher, fa, fb, *leases[5])
+    assert strip(again) == strip(list(compute_leases(matcher, fa, fb, leases[5:]))[0])
+
+
 def test_high_magnitude_canaries(runtime, focuses619):
     """N613 at p=613 and two cubes at p=619, each alone in a narrow interval
     (tools/run_production.py:102-105)."""
