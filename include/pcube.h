@@ -207,17 +207,23 @@ int pc_run_plain(pc_ctx *ctx, const pc_filters *filters, const pc_buf *us, uint6
 
 /*
  * Plain per-tile matcher that allocates no device memory (no counterpart in the reference).
- * For callers that cannot call cudaMalloc: code that runs while a stream is being captured into
- * a CUDA graph (allocation is refused there), code embedded in a process whose allocator already
- * owns the device's memory, and code that must not pay cudaMalloc's implicit device
- * synchronisation.  Same result as pc_run_plain with host inputs: us[nu], vs[nv] (sorted focus
- * values of one tile), the residual filters as for pc_filters_create, counts [ng+3] and
- * out [out_cap x 2] on the host.  Its scratch is a 16 MiB static device array inside the
- * library: inputs, filter tables and outputs must fit in it, or the call returns PC_INVALID with
- * the reason in err.  The first call on a device looks up the array's address (make that first
- * call before any stream capture).  It works on the legacy default stream; every call reuses the
- * same array, so calls that overlap on one GPU race with each other.  err (err_len bytes, may be
- * NULL) receives a message on failure.
+ * For callers that cannot call cudaMalloc: code embedded in a process whose own allocator has
+ * already taken the device's memory (a pool sized to the whole GPU leaves nothing for a library
+ * to allocate), and code that must not pay cudaMalloc's implicit device synchronisation in the
+ * middle of other work.  Same result as pc_run_plain with host inputs: us[nu], vs[nv] (sorted
+ * focus values of one tile), the residual filters as for pc_filters_create (primes and allowed
+ * must not be NULL), counts [ng+3] and out [out_cap x 2] on the host (out may be NULL only when
+ * out_cap is 0).  Its scratch is a 16 MiB static device array inside the library, held by every
+ * GPU that loads it until the process exits: inputs, filter tables and outputs must fit in it
+ * (at most 2^21 u or v entries, 2^20 output records, and their sum with the tables within
+ * 16 MiB), or the call returns PC_INVALID with the reason in err before touching the device.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current and caches it; make that first call before any stream capture, and do not
+ * call the entry point again on a device the process has reset.  The call selects `device` for
+ * its own work and restores the caller's current device before it returns.  It works on the
+ * legacy default stream and clears the counters it reads; every call reuses the same array, so
+ * calls that overlap on one GPU race with each other.  err (err_len bytes, may be NULL) receives
+ * a message on failure.
  */
 int pc_run_plain_static(int device, const uint64_t *us, uint64_t nu, const uint64_t *vs, uint64_t nv,
                         uint64_t A, uint64_t B, uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1,

@@ -1911,13 +1911,25 @@ int static_cuda(char *err, int err_len, cudaError_t e, const char *what) {
 }
 }  // namespace
 
+// The body of pc_run_plain_static once its device is current.
+static int plain_static_on(int device, const uint64_t *us, uint64_t nu, const uint64_t *vs, uint64_t nv, uint64_t A,
+                    uint64_t B, uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1, const uint32_t *primes,
+                    uint32_t nres, const uint8_t *allowed, uint32_t ng, uint64_t o_counts, uint64_t o_fc,
+                    uint64_t o_bits, uint64_t o_us, uint64_t o_vs, uint64_t o_out, uint64_t *counts, uint64_t *out,
+                    uint64_t out_cap, char *err, int err_len);
+
 extern "C" int pc_run_plain_static(int device, const uint64_t *us, uint64_t nu, const uint64_t *vs, uint64_t nv,
                                    uint64_t A, uint64_t B, uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1,
                                    const uint32_t *primes, uint32_t nres, const uint8_t *allowed, uint64_t *counts,
                                    uint64_t *out, uint64_t out_cap, char *err, int err_len) {
     if (device < 0 || device >= STATIC_MAX_DEVICES) return static_fail(err, err_len, PC_INVALID, "device index out of range");
-    if (nres == 0 || nres > PC_MAX_RES || A == 0 || B == 0 || !counts || (nu && !us) || (nv && !vs))
+    if (nres == 0 || nres > PC_MAX_RES || A == 0 || B == 0 || !counts || !primes || !allowed || (nu && !us) ||
+        (nv && !vs) || (out_cap && !out))
         return static_fail(err, err_len, PC_INVALID, "invalid plain tile arguments");
+    // every size is bounded by the scratch before any offset is formed, so no product below wraps
+    constexpr uint64_t too_big = STATIC_SCRATCH_BYTES;
+    if (nu > too_big / 8 || nv > too_big / 8 || out_cap > too_big / 16)
+        return static_fail(err, err_len, PC_INVALID, "tile exceeds the 16 MiB static scratch of pc_run_plain_static");
     uint64_t words = 0;
     for (uint32_t i = 0; i < nres; ++i) {
         const uint32_t q = primes[i];
@@ -1933,9 +1945,33 @@ extern "C" int pc_run_plain_static(int device, const uint64_t *us, uint64_t nu, 
     if (need > STATIC_SCRATCH_BYTES)
         return static_fail(err, err_len, PC_INVALID, "tile exceeds the 16 MiB static scratch of pc_run_plain_static");
 
-    cudaError_t e = cudaSetDevice(device);
-    if (e != cudaSuccess) return static_cuda(err, err_len, e, "cudaSetDevice");
-    if (!g_static_ptr[device]) {          // set-up, once per device, with that device current
+    // the caller's current device is put back on every return
+    int previous = -1;
+    cudaError_t e = cudaGetDevice(&previous);
+    if (e != cudaSuccess) return static_cuda(err, err_len, e, "cudaGetDevice");
+    if (previous != device) {
+        e = cudaSetDevice(device);
+        if (e != cudaSuccess) return static_cuda(err, err_len, e, "cudaSetDevice");
+    }
+    const int rc = plain_static_on(device, us, nu, vs, nv, A, B, lo0, lo1, hi0, hi1, primes, nres, allowed, ng,
+                                   o_counts, o_fc, o_bits, o_us, o_vs, o_out, counts, out, out_cap, err, err_len);
+    if (previous != device) {
+        e = cudaSetDevice(previous);
+        if (e != cudaSuccess && rc == PC_OK) return static_cuda(err, err_len, e, "cudaSetDevice (restore)");
+    }
+    return rc;
+}
+
+static int plain_static_on(int device, const uint64_t *us, uint64_t nu, const uint64_t *vs, uint64_t nv, uint64_t A,
+                    uint64_t B, uint64_t lo0, uint64_t lo1, uint64_t hi0, uint64_t hi1, const uint32_t *primes,
+                    uint32_t nres, const uint8_t *allowed, uint32_t ng, uint64_t o_counts, uint64_t o_fc,
+                    uint64_t o_bits, uint64_t o_us, uint64_t o_vs, uint64_t o_out, uint64_t *counts, uint64_t *out,
+                    uint64_t out_cap, char *err, int err_len) {
+    cudaError_t e = cudaSuccess;
+    // Set-up, once per device, with that device current.  The cached address belongs to the
+    // device's primary context; a process that resets the device (cudaDeviceReset) must not call
+    // this entry point on it again.
+    if (!g_static_ptr[device]) {
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_static_scratch);
         if (e != cudaSuccess) return static_cuda(err, err_len, e, "cudaGetSymbolAddress");

@@ -1,9 +1,9 @@
 """Regenerate the golden fixtures in this directory from the reference project.
 
-Run from the repository root in a container where the reference tree is mounted:
+Run from the repository root with the path of the reference project's tree:
 
-    python tests/golden/make_golden.py /root/reference
-    python tests/golden/make_golden.py /root/reference --cube-roots-only    # cube_roots.json alone
+    python tests/golden/make_golden.py <reference tree>
+    python tests/golden/make_golden.py <reference tree> --cube-roots-only    # cube_roots.json alone
 
 It imports the reference's own Python (pseudocube.focus / oracle / tables / accounting,
 review.verify_cube) from a scratch copy, runs the reference's compiled review tools from
@@ -236,7 +236,9 @@ def main(reference: Path) -> None:
 
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
-    ref = Path(args[0] if args else '/root/reference')
+    if not args:
+        raise SystemExit('usage: make_golden.py <reference tree> [--cube-roots-only]')
+    ref = Path(args[0])
     if '--cube-roots-only' in sys.argv:
         cube_root_fixtures(ref)
     else:
