@@ -332,11 +332,13 @@ __global__ void k_blocks(const VRec *__restrict__ rec, const SegDev *__restrict_
     pieces[b] = vb > va ? vb - va : 0;
 }
 
-// v chunk per work item: fixed, or total pieces / target items (at least 64, at most 2^20).
+// v chunk per work item: fixed, or total pieces / target items, at least min_chunk (two rounds of
+// 32 rows for every warp of a k_match CTA, so a small launch does not leave warps idle) and at
+// most 2^20.
 __global__ void k_chunk(const uint64_t *__restrict__ total_pieces, uint64_t fixed_chunk, uint64_t target_items,
-                        uint64_t *__restrict__ vchunk) {
+                        uint64_t min_chunk, uint64_t *__restrict__ vchunk) {
     uint64_t c = fixed_chunk;
-    if (!c) c = umax64((*total_pieces + target_items - 1) / umax64(1, target_items), 64);
+    if (!c) c = umax64((*total_pieces + target_items - 1) / umax64(1, target_items), min_chunk);
     *vchunk = umin64(c, UINT64_C(1) << 20);
 }
 
@@ -519,8 +521,14 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     // Items are handed out in ascending order from one device counter, so the CTAs work on
     // neighbouring blocks together: the per-v records of those blocks stay in L2, and the CTAs
     // finish within one grab of each other.  A grab takes as many items as a block averages (at
-    // least ITEM_GRAB), so a block cut into several items is mostly built by one CTA once.
-    const uint64_t grab = umax64(ITEM_GRAB, n_items / umax64(1, a.nblocks));
+    // least ITEM_GRAB), so a block cut into several items is mostly built by one CTA once, but
+    // never more than a quarter of an even share, so every CTA gets work.  A launch of fewer than
+    // eight items per CTA (one batch) gives each CTA one even share of consecutive items, which
+    // mostly lie in one block, so the rows of a block are built about once per CTA that meets it.
+    const uint64_t ncta = gridDim.x;
+    const uint64_t grab = n_items >= 8 * ncta
+                              ? umax64(ITEM_GRAB, umin64(n_items / umax64(1, a.nblocks), n_items / (4 * ncta)))
+                              : umax64(1, (n_items + ncta - 1) / ncta);
     uint64_t it = 0, it_end = 0;
     for (;;) {
         if (it == it_end) {
@@ -1281,7 +1289,8 @@ int engine_front(Engine &E, bool events, bool capturing, int *launches) {
     PC_LAUNCHED(ctx, "blocks");
     int rc = pc_exclusive_scan_ws(ctx, E.d_pieces, E.d_tmp, E.nblocks, E.d_tmp + E.nblocks, E.d_ws);
     if (rc) return rc;
-    k_chunk<<<1, 1, 0, st>>>(E.d_tmp + E.nblocks, E.tn.v_chunk, (uint64_t)E.grid * 32, E.d_vchunk);
+    k_chunk<<<1, 1, 0, st>>>(E.d_tmp + E.nblocks, E.tn.v_chunk, (uint64_t)E.grid * 32, 2 * (uint64_t)E.tn.threads,
+                             E.d_vchunk);
     PC_LAUNCHED(ctx, "chunk");
     k_item_counts<<<(unsigned)((E.nblocks + 255) / 256), 256, 0, st>>>(E.d_pieces, E.nblocks, E.d_vchunk, E.d_items);
     PC_LAUNCHED(ctx, "item counts");

@@ -182,7 +182,12 @@ class GPUFocus:
 class Filters:
     """Residual filter tables of one config on the device, in the reference's filter order."""
 
-    def __init__(self, runtime: Runtime, config: Config) -> None:
+    def __init__(self, runtime: Runtime, config: Config, table: Any = None) -> None:
+        """``table`` replaces the residue table uploaded to the device: one byte per residue r of
+        each filter q (1 = allowed), concatenated in filter order.  The default is the allowed
+        residues of each filter; another table is how a qualification run checks that the host
+        re-verification catches wrong device tables (the reference mutates its device table for
+        that, tools/gpu_worker.py:96-103 of its release archive)."""
         self.runtime, self.config = runtime, config
         order = config.filter_order()
         if not order:
@@ -190,12 +195,15 @@ class Filters:
         self.order = order
         self.filter_groups = [order[i:i + 4] for i in range(0, len(order), 4)]
         self.ng = len(self.filter_groups)
-        table = []
-        for q in order:
-            ring = [0] * q
-            for a in allowed(q):
-                ring[a] = 1
-            table.extend(ring)
+        if table is None:
+            table = []
+            for q in order:
+                ring = [0] * q
+                for a in allowed(q):
+                    ring[a] = 1
+                table.extend(ring)
+        elif len(table) != sum(order):
+            raise ValueError('residue table must hold one byte per residue of every filter')
         handle = ctypes.c_void_p()
         runtime.call(runtime.lib.pc_filters_create(runtime.ctx, config.A, config.B,
                                                    np.array(order, dtype=np.uint32), len(order),

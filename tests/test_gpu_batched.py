@@ -1,13 +1,14 @@
 """GPU parity of the batched form: many windows with different prime bounds, foci and intervals in
-one launch sequence, each checked against the plain per-tile path of the same build and, where the
-reference holds a fixture, against it; graph replays must equal the eager run."""
+one launch sequence, each checked against the oracle, against the plain per-tile path of the same
+build and, where the reference holds a fixture, against it; graph replays must equal the eager
+run."""
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
 from conftest import golden
-from psuedocubes_b200.batched import Autotuner, BatchedEngine, Window, seeded_windows
+from psuedocubes_b200.batched import WORKLOAD_PRIMES, Autotuner, BatchedEngine, Window, seeded_windows
 from psuedocubes_b200.batch_experiment import MaskedMatcher
 from psuedocubes_b200.focus import B619
 from psuedocubes_b200.gpu import Matcher
@@ -50,6 +51,28 @@ def test_mixed_prime_bounds_match_plain_path(runtime, engine):
         assert_same(row, plain(runtime, engine, w, 100_000_000))
     assert rows[3]['valid_focused_candidates'] > 10**9
     batch.close()
+
+
+def test_every_workload_prime_matches_oracle(runtime, engine, oracle, oracle619):
+    """24 seeded windows of the batched workload's span distribution, their prime bounds cycling
+    through every p of the workload (499 ... 619), in one launch sequence: every window's
+    populations, filter groups and complete sorted output against the oracle's masked batch over
+    the same Geometry (the A619/B619 focus tables do not depend on p)."""
+    _, ofa, ofb = oracle619
+    spans = seeded_windows(24, seed=499, span_exp=(6.0, 9.7))
+    windows = [Window(WORKLOAD_PRIMES[i % len(WORKLOAD_PRIMES)], w.first, w.end) for i, w in enumerate(spans)]
+    batch = engine.plan(windows, width=1 << 27)
+    batch.run()
+    rows = batch.results()
+    batch.close()
+    for w, row in zip(windows, rows):
+        g = oracle.Geometry(w.p, w.lo, w.hi, w.A, w.B)
+        want = oracle.batch(g, ofa, ofb, w.first, w.end, width=-(-(w.end - w.first) // 64), output_cap=1 << 16)
+        for key in ('valid_focused_candidates', 'group_survivors', 'filter_groups', 'local_survivors',
+                    'genuine_cubes'):
+            assert row[key] == want[key], (w, key)
+        assert sorted(int(n) for n in row['all_values']) == sorted(int(n) for n in want['all_values']), w
+    assert sum(row['valid_focused_candidates'] for row in rows) > 10**9
 
 
 def test_subtile_width_does_not_change_window_results(runtime, engine):

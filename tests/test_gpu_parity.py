@@ -253,6 +253,39 @@ def test_plain_batch_equals_masked(runtime, p619, focuses619):
         assert plain[key] == masked[key], key
 
 
+@pytest.mark.parametrize('case', ['p499', 'p613', 'p571-request-split'])
+def test_plain_tiles_match_oracle(runtime, focuses619, oracle, oracle619, case):
+    """The plain matcher (the baseline of the batched and served forms) against the oracle's plain
+    tile at prime bounds other than 619, and with a focus split the served planner chooses."""
+    from psuedocubes_b200.served import plan_request
+    if case == 'p571-request-split':
+        lo, hi = 2 * 10**27, 2 * 10**27 + 10**17
+        plan = plan_request(571, lo, hi)
+        c = Config(571, lo, hi, plan.A, plan.B)
+        fa, fb = (GPUFocus(runtime, f) for f in c.focuses())
+        g = oracle.Geometry(571, lo, hi, plan.A, plan.B)
+        ofa, ofb = oracle.OracleFocus(g, 'A'), oracle.OracleFocus(g, 'B')
+        tile = Tile(plan.B // 3, plan.B // 3 + plan.B // 2000)       # within the 5e7 pair limit
+    else:
+        p = int(case[1:])
+        c = Config(p, 10**27, 3 * 10**27, A619, B619)
+        fa, fb = focuses619
+        _, ofa, ofb = oracle619
+        g = oracle.Geometry(p, c.lo, c.hi, A619, B619)
+        tile = Tile(658625401600000000, 658625401600000000 + 100_000_000)
+    got = Matcher(runtime, c).tile(tile, fa, fb, output_cap=1 << 16)
+    us = ofa.window(c.u_interval(tile.first)[0], c.u_interval(tile.end - 1)[1], cap=1 << 30)
+    vs = ofb.window(tile.first, tile.end, cap=1 << 30)
+    want = oracle.plain_tile(g, us, vs, output_cap=1 << 16)
+    ng = len(g.filter_groups)
+    pops = want['populations']
+    assert got['focus_u'] == len(us) and got['focus_v'] == len(vs)
+    assert got['valid_focused_candidates'] == pops[0] > 0
+    assert got['group_survivors'] == pops[1:ng + 1]
+    assert got['local_survivors'] == pops[ng + 1] and pops[ng + 2] == 0
+    assert [int(n) for n in got['all_values']] == want['values']
+
+
 def test_p67_prefix(runtime, oracle):
     case = golden('p67_prefix.json')
     c = Config(67, 1, 10**13, case['A'], case['B'])
@@ -277,9 +310,10 @@ def test_coordinates_upload_roundtrip(runtime):
     assert arr[1:3].searchsorted([0, 5, 6, 2**64 - 1]).tolist() == [0, 0, 1, 2]
 
 
-@pytest.mark.parametrize('index', [0, 3])
+@pytest.mark.parametrize('index', [0, 3, 24])
 def test_bench_lease_batches_match_oracle(runtime, p619, focuses619, oracle, oracle619, index):
-    """The leases bench.py times (its warm-up lease 0 and first timed lease 3): the first, a middle
+    """Leases bench.py times: lease 0 (its first warm-up lease), 3 (the first timed lease at its
+    default --warmup 3) and 24 (the last timed lease at --warmup 5 --steps 20): the first, a middle
     and the last batch of each, subtile by subtile, against the oracle."""
     import bench
     fa, fb = focuses619
@@ -299,3 +333,27 @@ def test_bench_lease_batches_match_oracle(runtime, p619, focuses619, oracle, ora
             assert oracle.digest([str(n) for n in raw['per_tile'][t]]) == scope['output_sha256']
         geo = raw['geometry'][64 * b:64 * b + 64]
         assert int(geo[:, 0].sum()) == want['focus_u'] and int(geo[:, 1].sum()) == want['focus_v']
+
+
+@pytest.mark.parametrize('index', [5, 25])
+def test_bench_leases_match_oracle_whole(runtime, p619, focuses619, oracle, oracle619, index):
+    """At --warmup 5 --steps 20, lease 5 is the first lease bench.py times on the device and lease
+    25 the first of its end-to-end run through compute_leases.  Each is checked whole against the
+    oracle's lease: all 256 batches, through the transcript over 16,384 subtile scopes, the
+    output hash, the populations and the values."""
+    import os
+    import bench
+    fa, fb = focuses619
+    g, ofa, ofb = oracle619
+    first, end = bench.lease_bounds(index)
+    got = compute_lease(MaskedMatcher(runtime, p619), fa, fb, first, end)
+    workers = max(1, (os.cpu_count() or 2) // 2)
+    want = oracle.lease(g, ofa, ofb, first, end, workers=workers, threads_per_batch=2)
+    scope = got['subtile_scopes'][0]
+    assert scope['transcript_sha256'] == want['transcript_sha256']
+    assert scope['output_sha256'] == want['output_sha256']
+    for key in ('focus_u', 'focus_v', 'cartesian_opportunities', 'valid_focused_candidates', 'genuine_cubes',
+                'local_survivors', 'group_survivors', 'filter_groups', 'all_values', 'compute_batches',
+                'subtiles_executed'):
+        assert got[key] == want[key], key
+    assert [h['n'] for h in got['cpu_confirmed_hits']] == [h['n'] for h in want['cpu_confirmed_hits']]

@@ -47,6 +47,25 @@ def test_served_equals_the_plain_per_request_loop(runtime, mixed):
             assert got[key] == want[key], (r.id, key)
 
 
+def test_served_requests_match_oracle(mixed, oracle):
+    """Three requests, each against the oracle's masked batch over the whole canonical domain
+    [0, B') of the request's own focus split (A', B') from the planner: populations, filter groups,
+    the complete sorted output and its digest."""
+    for r in (REQUESTS[0], REQUESTS[1], REQUESTS[4]):
+        got = mixed['results'][r.id]
+        A, B = int(got['A']), int(got['B'])
+        g = oracle.Geometry(r.p, r.lo, r.hi, A, B)
+        fa, fb = oracle.OracleFocus(g, 'A'), oracle.OracleFocus(g, 'B')
+        want = oracle.batch(g, fa, fb, 0, B, width=-(-B // 64), output_cap=1 << 16)
+        for key in ('valid_focused_candidates', 'group_survivors', 'filter_groups', 'local_survivors',
+                    'genuine_cubes'):
+            assert got[key] == want[key], (r.id, key)
+        values = sorted(int(n) for n in want['all_values'])
+        assert got['values'] == values, r.id
+        assert got['output_sha256'] == oracle.digest([str(n) for n in values]), r.id
+        assert got['valid_focused_candidates'] > 10**9
+
+
 def test_output_set_does_not_depend_on_the_focus_split(runtime, mixed):
     r = REQUESTS[0]
     plan = plan_request(r.p, r.lo, r.hi)
