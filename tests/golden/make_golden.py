@@ -4,6 +4,7 @@ Run from the repository root with the path of the reference project's tree:
 
     python tests/golden/make_golden.py <reference tree>
     python tests/golden/make_golden.py <reference tree> --cube-roots-only    # cube_roots.json alone
+    python tests/golden/make_golden.py <reference tree> --focus-only         # focus.json alone
 
 It imports the reference's own Python (pseudocube.focus / oracle / tables / accounting,
 review.verify_cube) from a scratch copy, runs the reference's compiled review tools from
@@ -68,6 +69,53 @@ def cube_root_fixtures(reference: Path) -> None:
         counted.append(dict(first=a, last=b, p=p, count=int(rows[0]['count'])))
     dump('cube_roots.json', dict(recorded=recorded, listed=listed, counted=counted,
                                  list_digest='sha256 of the ascending decimal roots joined by commas'))
+
+
+def focus_fixtures(reference: Path) -> None:
+    """The reference's pseudocube.focus on five configurations (p = 619 production, the p = 67
+    split, the p = 31, 13 and 7 small sets): manifests, filter order, rings, terms digests, halves,
+    seeded at/rank/indices samples, canonical pairs, u intervals, tile manifests and splits, and
+    factors() answers (ring moduli or the error message) on accepted and refused moduli."""
+    scratch = Path(tempfile.mkdtemp(prefix='pcube-ref-'))
+    shutil.copytree(reference / 'pseudocube', scratch / 'pseudocube')
+    sys.path.insert(0, str(scratch))
+    from pseudocube.focus import A619, B619, Config, Tile, factors
+    rng = random.Random(619003)
+    configs = []
+    for p, lo, hi, A, B in ((619, 10**27, 3 * 10**27, A619, B619), (67, 1, 10**13, 2523326, 2486169),
+                            (31, 0, 100000, 266, 3627), (13, 0, 100000, 14, 117), (7, 0, 100000, 14, 9)):
+        c = Config(p, lo, hi, A, B)
+        row = dict(p=p, lo=str(lo), hi=str(hi), A=str(A), B=str(B), manifest=c.manifest(),
+                   residuals=c.residuals(), foci=[])
+        for focus in c.focuses():
+            at = [(i, focus.at(i)) for i in sorted(rng.randrange(focus.count) for _ in range(64))]
+            coords = [focus.at(rng.randrange(focus.count)) + rng.randrange(3) * focus.modulus for _ in range(64)]
+            start = rng.randrange(max(1, focus.count - 40))
+            first, second = focus.halves()
+            row['foci'].append(dict(
+                modulus=str(focus.modulus), count=str(focus.count), rings=[[q, list(r)] for q, r in focus.rings],
+                terms_sha256=hashlib.sha256(json.dumps([[str(t) for t in ts] for ts in focus.terms]).encode()).hexdigest(),
+                halves=[[len(t) for t in first], [len(t) for t in second]],
+                at=[[str(i), str(v)] for i, v in at], rank=[[str(x), [str(k) for k in focus.rank(x)]] for x in coords],
+                indices=dict(start=start, end=min(focus.count, start + 40), period=2,
+                             values=[str(x) for x in focus.indices(start, min(focus.count, start + 40), 2)])))
+        row['canonical'] = []
+        for n in [lo + 1, hi, *(rng.randrange(lo + 1, hi + 1) for _ in range(64))]:
+            u, v = c.canonical(n)
+            row['canonical'].append([str(n), str(u), str(v), *(str(x) for x in c.u_interval(v))])
+        t = Tile(rng.randrange(B // 2), B)
+        row['tile'] = dict(first=str(t.first), end=str(t.end), manifest=t.manifest(c),
+                           split=[[str(x.first), str(x.end)] for x in t.split()])
+        configs.append(row)
+    answers = []
+    for n, p in ((14, 7), (9, 7), (3, 7), (27 * 5, 7), (9 * 49, 7), (9 * 11, 7), (8 * 7, 13), (10**19, 7),
+                 (0, 7), (1, 7), (A619, 619), (B619, 619), (A619, 179), (9 * 7 * 13 * 31, 31)):
+        try:
+            answers.append(dict(n=str(n), p=p, rings=factors(n, p)))
+        except ValueError as exc:
+            answers.append(dict(n=str(n), p=p, error=str(exc)))
+    dump('focus.json', dict(configs=configs, factors=answers))
+    shutil.rmtree(scratch)
 
 
 def main(reference: Path) -> None:
@@ -241,5 +289,8 @@ if __name__ == '__main__':
     ref = Path(args[0])
     if '--cube-roots-only' in sys.argv:
         cube_root_fixtures(ref)
+    elif '--focus-only' in sys.argv:
+        focus_fixtures(ref)
     else:
         main(ref)
+        focus_fixtures(ref)

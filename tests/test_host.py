@@ -2,6 +2,8 @@
 from __future__ import annotations
 
 import ctypes
+import hashlib
+import json
 import re
 
 import numpy as np
@@ -264,3 +266,38 @@ def test_overlapped_leases_issue_ahead_and_keep_order(p619):
         assert strip(receipt) == strip(compute_lease(FakeLeases(), None, None, first, end))
     with pytest.raises(ArithmeticError):
         list(compute_leases(FakeLeases(), None, None, [(0, width), (666, 666 + width)]))
+
+
+def test_focus_module_matches_reference_fixtures():
+    """Config, Focus, Tile and factors against the reference's pseudocube.focus on five
+    configurations (tests/golden/focus.json, written by make_golden.py from the reference)."""
+    from psuedocubes_b200.focus import Tile, factors
+    fx = golden('focus.json')
+    for row in fx['configs']:
+        c = Config(row['p'], int(row['lo']), int(row['hi']), int(row['A']), int(row['B']))
+        assert c.manifest() == row['manifest'] and c.residuals() == row['residuals']
+        for focus, want in zip(c.focuses(), row['foci']):
+            assert str(focus.modulus) == want['modulus'] and str(focus.count) == want['count']
+            assert [[q, list(r)] for q, r in focus.rings] == want['rings']
+            terms = hashlib.sha256(json.dumps([[str(t) for t in ts] for ts in focus.terms]).encode()).hexdigest()
+            assert terms == want['terms_sha256']
+            first, second = focus.halves()
+            assert [[len(t) for t in first], [len(t) for t in second]] == want['halves']
+            for i, v in want['at']:
+                assert str(focus.at(int(i))) == v
+            for x, (period, index) in want['rank']:
+                assert focus.rank(int(x)) == (int(period), int(index))
+                assert focus.contains(int(x))
+            w = want['indices']
+            assert [str(x) for x in focus.indices(w['start'], w['end'], w['period'])] == w['values']
+        for n, u, v, lo, hi in row['canonical']:
+            assert c.canonical(int(n)) == (int(u), int(v)) and c.u_interval(int(v)) == (int(lo), int(hi))
+        t = Tile(int(row['tile']['first']), int(row['tile']['end']))
+        assert t.manifest(c) == row['tile']['manifest']
+        assert [[str(x.first), str(x.end)] for x in t.split()] == row['tile']['split']
+    for case in fx['factors']:
+        if 'rings' in case:
+            assert factors(int(case['n']), case['p']) == case['rings']
+        else:
+            with pytest.raises(ValueError, match=re.escape(case['error'])):
+                factors(int(case['n']), case['p'])
