@@ -33,7 +33,8 @@ from typing import Any, Iterable
 import numpy as np
 
 from . import _native as N
-from .batch_experiment import batch_result
+from .accounting import EMPTY_DIGEST, digest
+from .batch_experiment import verify_values
 from .focus import A619, B619, Config
 from .gpu import MASK, Filters, GPUFocus, Runtime
 
@@ -223,29 +224,63 @@ class WindowBatch:
         return int(counts[:, 0].sum())
 
     def results(self) -> list[dict[str, Any]]:
-        """Per-window results of the last run, host-verified like the reference's tile results."""
+        """Per-window results of the last run, host-verified like the reference's tile results
+        (the fields of batch_experiment.batch_result).  Counters of all windows are reduced in a
+        few array passes; only windows that emitted values touch them one by one."""
         counts, geometry, records = self.raw()
-        tile = (records[:, 1] >> np.uint64(32)).astype(np.int64) if len(records) else np.zeros(0, dtype=np.int64)
-        lo = records[:, 0] if len(records) else np.zeros(0, dtype=np.uint64)
-        hi = records[:, 1] & np.uint64(0xFFFFFFFF) if len(records) else np.zeros(0, dtype=np.uint64)
+        n, nt = len(self.windows), self.ntiles
+        tb = self.tile_base.astype(np.int64)
+        ngs = np.array([self.families[self._family_of[i]].ng for i in range(n)], dtype=np.int64)
+        tile_ng = np.repeat(ngs, np.diff(tb))
+        at = np.arange(nt)
+        emitted = counts[at, tile_ng + 1]
+        if np.any(counts[at, tile_ng + 2]):
+            raise ArithmeticError('unsigned underflow')
+        tile = (records[:, 1] >> np.uint64(32)).astype(np.int64)
+        if len(tile) and (tile.min() < 0 or tile.max() >= nt):
+            raise ArithmeticError('output record outside the launch')
+        if not np.array_equal(np.bincount(tile, minlength=nt), emitted.astype(np.int64)):
+            raise ArithmeticError('device output count disagrees with its records')
+        order = np.argsort(tile, kind='stable')
+        tile_sorted = tile[order]
+        lo_limb, hi_limb = records[order, 0], records[order, 1] & np.uint64(0xFFFFFFFF)
+        cuts = np.searchsorted(tile_sorted, np.arange(nt + 1))
+        valid = counts[:, 0].tolist()
+        emitted_list = emitted.tolist()
+        table = counts.tolist()
+        sums = np.add.reduceat(counts, tb[:-1], axis=0).tolist() if nt else [[0] * self.stride] * n
+        gu, gv = geometry[:, 0].tolist(), geometry[:, 1].tolist()
         out = []
         for i, (w, c) in enumerate(zip(self.windows, self.configs)):
-            t0, t1 = int(self.tile_base[i]), int(self.tile_base[i + 1])
-            fam = self.families[self._family_of[i]]
-            ng = fam.ng
-            pops = counts[t0:t1, :ng + 3]
-            per_tile: list[list[int]] = [[] for _ in range(t1 - t0)]
-            for k in np.nonzero((tile >= t0) & (tile < t1))[0].tolist():
-                per_tile[int(tile[k]) - t0].append(int(lo[k]) | (int(hi[k]) << 64))
-            for values in per_tile:
-                values.sort()
-            ranges = []                                   # subtile v ranges (the u bounds are not read)
-            for v in range(w.first, w.end, self.widths[i]):
-                ranges.append((v, min(v + self.widths[i], w.end), 0, 0))
-            geo = [(int(a), int(b)) for a, b in geometry[t0:t1]]
-            row = batch_result(c, ranges, pops, per_tile, geo, fam.filter_groups, 1 << 62)
-            row.update(p=w.p, first=str(w.first), end=str(w.end), focus_u=int(self.sizes[2 * i]),
-                       focus_v=int(self.sizes[2 * i + 1]))
+            t0, t1, ng = int(tb[i]), int(tb[i + 1]), int(ngs[i])
+            width = self.widths[i]
+            group_rows = [row[1:ng + 1] for row in table[t0:t1]]
+            firsts = range(w.first, w.end, width)
+            digests, values = [EMPTY_DIGEST] * (t1 - t0), []
+            for t in range(t0, t1):
+                if not emitted_list[t]:
+                    continue
+                k0, k1 = int(cuts[t]), int(cuts[t + 1])
+                tile_values = sorted(int(a) | int(b) << 64 for a, b in zip(lo_limb[k0:k1].tolist(), hi_limb[k0:k1].tolist()))
+                first = w.first + (t - t0) * width
+                end = min(first + width, w.end)
+                if any(not first <= c.canonical(x)[1] < end for x in tile_values):
+                    raise ArithmeticError('output assigned to wrong subtile')
+                digests[t - t0] = digest([str(x) for x in tile_values])
+                values.extend(tile_values)
+            hits = verify_values(c, values) if values else []
+            scopes = [dict(first=str(f), end=str(min(f + width, w.end)), valid_focused_candidates=v,
+                           group_survivors=g, local_survivors=e, output_sha256=d)
+                      for f, v, g, e, d in zip(firsts, valid[t0:t1], group_rows, emitted_list[t0:t1], digests)]
+            us, vs = gu[t0:t1], gv[t0:t1]
+            row = dict(status='PASS', host_verified=True, focus_u=int(self.sizes[2 * i]),
+                       focus_v=int(self.sizes[2 * i + 1]), cartesian_opportunities=sum(a * b for a, b in zip(us, vs)),
+                       valid_focused_candidates=sum(valid[t0:t1]), genuine_cubes=len(values) - len(hits),
+                       local_survivors=len(values), cube_checks=len(values), subtile_scopes=scopes,
+                       filter_groups=self.families[self._family_of[i]].filter_groups,
+                       group_survivors=sums[i][1:ng + 1] if t1 > t0 else [0] * ng,
+                       all_values=[str(x) for x in values], cpu_confirmed_hits=hits, overflow_splits=[],
+                       p=w.p, first=str(w.first), end=str(w.end))
             out.append(row)
         return out
 

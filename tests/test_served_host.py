@@ -128,3 +128,65 @@ def test_scheduler_runs_every_window_once():
     type(loop).control = 1                           # a control that disagrees with what was emitted
     with pytest.raises(ArithmeticError):
         loop.run(reqs[:1], realtime=False)
+
+
+def test_window_results_equal_per_window_batch_results():
+    """WindowBatch.results() reduces the counters of all windows at once; it must give, window by
+    window, the fields batch_experiment.batch_result gives for the same counters and records (here
+    synthetic counters and the golden lease's 82 real survivors placed in their subtiles)."""
+    import types
+    import numpy as np
+    from conftest import golden
+    from psuedocubes_b200.batch_experiment import batch_result
+    from psuedocubes_b200.batched import Window, WindowBatch
+    from psuedocubes_b200.focus import A619, B619, Config
+    gold = golden('golden_lease.json')
+    g0, g1 = int(gold['first']), int(gold['end'])
+    values = [int(n) for n in gold['result']['all_values']]
+    windows = [Window(619, g0, g1), Window(499, 5, 5 + 3 * 10**8 + 7), Window(613, B619 - 10**9, B619),
+               Window(571, 10**15, 10**15 + 1)]
+    widths = [10**8, 1 << 27, 10**8, 10**8]
+    configs = [w.config() for w in windows]
+    ntiles = [-(-(w.end - w.first) // wd) for w, wd in zip(windows, widths)]
+    fams = {}
+    for c in configs:
+        groups = c.filter_groups()
+        fams.setdefault(c.p, types.SimpleNamespace(ng=len(groups), filter_groups=groups))
+    families = list(fams.values())
+    b = object.__new__(WindowBatch)
+    b.windows, b.configs, b.widths = windows, configs, widths
+    b.families = families
+    b._family_of = [families.index(fams[c.p]) for c in configs]
+    b.tile_base = np.array([0, *np.cumsum(ntiles)], dtype=np.uint32)
+    b.ntiles = int(sum(ntiles))
+    b.stride = max(f.ng for f in families) + 3
+    b.sizes = np.array([x for k in range(len(windows)) for x in (1000 + k, 2000 + k)], dtype=np.uint64)
+    rng = np.random.default_rng(5)
+    counts = np.zeros((b.ntiles, b.stride), dtype=np.uint64)
+    counts[:, :b.stride - 2] = rng.integers(0, 10**9, size=(b.ntiles, b.stride - 2), dtype=np.uint64)
+    records = []
+    for n in values:                                      # the golden values, in window 0's subtiles
+        t = (configs[0].canonical(n)[1] - g0) // widths[0]
+        records.append((n & (2**64 - 1), n >> 64 | t << 32))
+    records = np.array(records, dtype=np.uint64)[rng.permutation(len(values))]
+    tile_ng = np.repeat([families[f].ng for f in b._family_of], ntiles)
+    counts[np.arange(b.ntiles), tile_ng + 1] = 0
+    counts[np.arange(b.ntiles), tile_ng + 2] = 0
+    np.add.at(counts, (records[:, 1] >> np.uint64(32)).astype(np.int64), 0)
+    for t in (records[:, 1] >> np.uint64(32)).astype(np.int64):
+        counts[t, tile_ng[t] + 1] += 1
+    geometry = rng.integers(0, 10**6, size=(b.ntiles, 2), dtype=np.uint64)
+    b.raw = lambda: (counts, geometry, records)
+    rows = b.results()
+    for i, (w, c) in enumerate(zip(windows, configs)):
+        t0, t1 = int(b.tile_base[i]), int(b.tile_base[i + 1])
+        ng = families[b._family_of[i]].ng
+        tiles = (records[:, 1] >> np.uint64(32)).astype(np.int64)
+        per_tile = [sorted(int(records[k, 0]) | int(records[k, 1] & np.uint64(0xFFFFFFFF)) << 64
+                           for k in np.nonzero(tiles == t)[0]) for t in range(t0, t1)]
+        ranges = [(v, min(v + widths[i], w.end), 0, 0) for v in range(w.first, w.end, widths[i])]
+        want = batch_result(c, ranges, counts[t0:t1, :ng + 3], per_tile, [(int(a), int(b_)) for a, b_ in geometry[t0:t1]],
+                            families[b._family_of[i]].filter_groups, 1 << 62)
+        want.update(p=w.p, first=str(w.first), end=str(w.end), focus_u=1000 + i, focus_v=2000 + i)
+        assert rows[i] == want, i
+    assert rows[0]['local_survivors'] == 82 and len(rows[0]['cpu_confirmed_hits']) == 1
