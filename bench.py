@@ -134,6 +134,10 @@ def cpu_sample(steps: int, warmup: int, batches: int = 16) -> dict:
     from oracle import pcube_oracle as O
     g = O.Geometry(619, 10**27, 3 * 10**27, O.A619, O.B619)
     fa, fb = O.OracleFocus(g, 'A'), O.OracleFocus(g, 'B')
+    # stage 1 through the reference's own CPU window producer (review/focus_window_cpu.cpp,
+    # compiled into oracle/_ref) where it was built; stages 2 and 3 are the C restatement
+    stage1 = 'reference' if O.reference_producer() is not None else 'port'
+    fa.producer = fb.producer = stage1
     first, _ = lease_bounds(warmup)
     cores = os.cpu_count() or 1
     positions, elapsed = 0, 0.0
@@ -144,8 +148,10 @@ def cpu_sample(steps: int, warmup: int, batches: int = 16) -> dict:
         elapsed += time.perf_counter() - t0
         positions += r['valid_focused_candidates']
     return dict(value=positions / elapsed, unit=UNIT, cores=cores, kind='port',
-                sample=f'{batches} consecutive p=619 batches ({batches * 64} subtiles) per step, {max(1, steps)} steps, '
-                       f'C restatement of the window producer and masked matcher, {cores} threads',
+                sample=f'{batches} consecutive p=619 batches ({batches * 64} subtiles) per step, {max(1, steps)} steps; '
+                       + ('stage 1 by the reference\'s focus_window_cpu.cpp' if stage1 == 'reference'
+                          else 'stage 1 by the C restatement of the window producer')
+                       + f', the masked matcher by the C restatement; {cores} threads',
                 seconds=elapsed, positions=positions)
 
 
@@ -210,7 +216,7 @@ def run_ours(args) -> None:
         step(k)
     barrier(dist)
     runtime.synchronize()
-    positions, kernel_ms, launches, outputs = 0, 0.0, 0, 0
+    positions, kernel_ms, launches, outputs, h2d, d2h_lib = 0, 0.0, 0, 0, 0, 0
     stage_ms = dict(window_ms=0.0, bounds_ms=0.0, kernel_ms=0.0)
     with ClockSampler(local) as clocks:
         runtime.call(lib.pc_mark(ctx, 0))
@@ -220,6 +226,8 @@ def run_ours(args) -> None:
             kernel_ms += st['kernel_ms']
             launches += st['launches']
             outputs += st['outputs']
+            h2d += st['h2d_bytes']
+            d2h_lib += st['d2h_bytes']
             for key in stage_ms:
                 stage_ms[key] += st[key] / args.steps
         runtime.call(lib.pc_mark(ctx, 1))
@@ -241,7 +249,9 @@ def run_ours(args) -> None:
     for result in compute_leases(matcher, af, bf, leases):
         e2e_positions += result['valid_focused_candidates']
     e2e_seconds = max_over_ranks(dist, time.perf_counter() - t0, local) if e2e_steps else 0.0
-    d2h = counts.nbytes + geometry.nbytes + 16 + 16 * (outputs // max(1, args.steps))
+    # the library's own count of the bytes one lease call copies (window and segment descriptors,
+    # subtile map up; counters, envelope sizes, records and scalars down), as in compute_leases
+    h2d_step, d2h_step = h2d // max(1, args.steps), d2h_lib // max(1, args.steps)
     if rank == 0:
         clock = clocks.summary()
         sm_mhz = clock['sm_max_mhz'] or 1965.0
@@ -261,8 +271,11 @@ def run_ours(args) -> None:
                                   kernel='k_match (fused bitset + 128-bit filters)',
                                   ops_per_position=OPS_PER_POSITION,
                                   peak_basis=f'{runtime.sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz'),
-                    e2e=dict(value=e2e_positions * world / e2e_seconds if e2e_seconds else None, unit=UNIT, h2d_bytes_per_step=0,
-                             d2h_bytes_per_step=int(d2h), api='psuedocubes_b200.optimized.compute_leases'),
+                    e2e=dict(value=e2e_positions * world / e2e_seconds if e2e_seconds else None, unit=UNIT,
+                             h2d_bytes_per_step=int(h2d_step), d2h_bytes_per_step=int(d2h_step),
+                             api='psuedocubes_b200.optimized.compute_leases',
+                             inputs='per lease: window, segment and subtile descriptors; the focus lists are '
+                                    'generated on the device from the resident wheel tables'),
                     gpu_launches=launches, clocks=clock, tuning=effective,
                     kernel_ms_per_step=kernel_ms / args.steps, stage_ms_per_step=stage_ms)
         if kernel_ms and effective.get('bitset_filters'):
@@ -397,9 +410,11 @@ def run_served(args) -> None:
     """Served range certification: Poisson arrivals at 20 requests/s of (p, x_lo, x_hi), p uniform
     over the accepted primes in [499, 619], x_lo = 10^U(20, log10 3e27), span = 10^U(15, 22),
     admitted by device memory under an 8 GiB cap, continuous batching; beside it the sequential
-    plain per-request loop on the same arrival stream, under a time limit."""
+    plain per-request loop on the same arrival stream, under a time limit.  Two more runs make the
+    comparison uncensored: the same distribution at a rate the device sustains (``--sustained-rate``),
+    and a sub-stream of the stream's small-span requests that both loops finish."""
     from psuedocubes_b200.gpu import Runtime
-    from psuedocubes_b200.served import ServedLoop, latency_summary, plain_loop, poisson_requests
+    from psuedocubes_b200.served import ServedLoop, latency_summary, plain_loop, poisson_requests, rescaled
 
     rank, world, local, dist = dist_setup(args.gpus)
     runtime = Runtime(time.monotonic() + 7200, 8 * 1024**3, 0.5, device=local)
@@ -407,6 +422,17 @@ def run_served(args) -> None:
     warm = [r for r in poisson_requests(40, rate=20.0, seed=7) if r.hi - r.lo <= 10**17][:3]
     ServedLoop(runtime).run(warm, realtime=False)
     barrier(dist)
+    keys = ('valid_focused_candidates', 'group_survivors', 'local_survivors', 'genuine_cubes', 'output_sha256')
+
+    def compare(a: dict, b: dict) -> tuple[int, int]:
+        compared = mismatches = 0
+        for rid, want in b['results'].items():
+            got = a['results'].get(rid)
+            if got is not None:
+                compared += 1
+                mismatches += any(got[k] != want[k] for k in keys)
+        return compared, mismatches
+
     loop = ServedLoop(runtime)
     with ClockSampler(local) as clocks:
         served = loop.run(requests, realtime=True, time_limit=args.served_limit)
@@ -414,17 +440,22 @@ def run_served(args) -> None:
     print(json.dumps(dict(served=served_summary, seconds=served['seconds'])), file=sys.stderr, flush=True)
     plain = plain_loop(runtime, requests, time_limit=args.plain_limit)
     plain_summary = latency_summary(plain, requests)
-    mismatches = compared = 0
-    for rid, want in plain['results'].items():
-        got = served['results'].get(rid)
-        if got is None:
-            continue
-        compared += 1
-        keys = ('valid_focused_candidates', 'group_survivors', 'local_survivors', 'genuine_cubes', 'output_sha256')
-        mismatches += any(got[k] != want[k] for k in keys)
+    compared, mismatches = compare(served, plain)
     kernel_ms = sum(s['kernel_ms'] for s in loop.steps)
     breakdown = {k: sum(s[k] for s in loop.steps) for k in ('window_ms', 'bounds_ms', 'kernel_ms', 'total_ms',
                                                              'u_entries', 'v_entries', 'positions', 'windows')}
+    # the same distribution at a load the device sustains: p50/p99 of the engine, not of a backlog
+    sustained_requests = poisson_requests(args.requests, rate=args.sustained_rate, seed=619003 + rank)
+    sustained_loop = ServedLoop(runtime)
+    sustained = sustained_loop.run(sustained_requests, realtime=True, time_limit=args.served_limit)
+    sustained_summary = latency_summary(sustained, sustained_requests)
+    sustained_ms = sum(s['kernel_ms'] for s in sustained_loop.steps)
+    # the stream's small-span requests, which the plain loop also finishes: both loops uncensored
+    small = rescaled([r for r in requests if r.hi - r.lo <= args.small_span][:args.small_requests], args.small_rate)
+    small_served = ServedLoop(runtime).run(small, realtime=True)
+    small_plain = plain_loop(runtime, small)
+    small_compared, small_mismatches = compare(small_served, small_plain)
+    steps = loop.steps + sustained_loop.steps
     if rank == 0:
         line = dict(metric=SERVED_METRIC, value=served_summary['positions_per_second'], unit=UNIT, n_gpus=world,
                     steps=len(loop.steps), warmup=len(warm), ms_per_step=1000 * served['seconds'] / max(1, len(loop.steps)),
@@ -437,11 +468,21 @@ def run_served(args) -> None:
                                 device_ms=kernel_ms, device_busy=kernel_ms / 1000 / served['seconds'],
                                 breakdown=breakdown),
                     plain_path=dict(plain_summary, seconds=plain['seconds'], positions=plain['positions'],
-                                    api='sequential plain per-request loop (Matcher.tile over the same windows)'),
+                                    api='sequential plain per-request loop (Matcher.tile over the same windows)',
+                                    note='censored: requests unfinished at the time limit count with the limit as '
+                                         'their latency, so p50/p99 are lower bounds' if plain_summary['censored'] else ''),
                     compared_requests=compared, mismatches=mismatches,
-                    e2e=dict(value=served_summary['positions_per_second'], unit=UNIT, h2d_bytes_per_step=None,
-                             d2h_bytes_per_step=None, api='ServedLoop.run (requests in, verified results out)'),
-                    gpu_launches=None, clocks=clocks.summary())
+                    sustained=dict(sustained_summary, rate=args.sustained_rate, seconds=sustained['seconds'],
+                                   positions=sustained['positions'], device_ms=sustained_ms,
+                                   device_busy=sustained_ms / 1000 / sustained['seconds']),
+                    small_spans=dict(requests=len(small), rate=args.small_rate, max_span=args.small_span,
+                                     served=latency_summary(small_served, small), plain=latency_summary(small_plain, small),
+                                     compared_requests=small_compared, mismatches=small_mismatches),
+                    e2e=dict(value=served_summary['positions_per_second'], unit=UNIT,
+                             h2d_bytes_per_step=int(sum(s.get('h2d_bytes', 0) for s in loop.steps) / max(1, len(loop.steps))),
+                             d2h_bytes_per_step=int(sum(s.get('d2h_bytes', 0) for s in loop.steps) / max(1, len(loop.steps))),
+                             api='ServedLoop.run (requests in, verified results out)'),
+                    gpu_launches=int(sum(s.get('launches', 0) for s in steps)), clocks=clocks.summary())
         print(json.dumps(line), flush=True)
     runtime.close()
     if dist is not None:
@@ -586,6 +627,12 @@ def main() -> None:
     parser.add_argument('--requests', type=int, default=100, help='served: requests in the arrival stream')
     parser.add_argument('--served-limit', type=float, default=240.0, help='served: seconds before the loop stops')
     parser.add_argument('--plain-limit', type=float, default=60.0, help='served: seconds for the plain loop')
+    parser.add_argument('--sustained-rate', type=float, default=2.0,
+                        help='served: arrival rate of the second run, one the device sustains')
+    parser.add_argument('--small-span', type=int, default=10**16,
+                        help='served: largest span of the small-span sub-stream both loops finish')
+    parser.add_argument('--small-requests', type=int, default=12, help='served: requests in the small-span sub-stream')
+    parser.add_argument('--small-rate', type=float, default=1.0, help='served: arrival rate of the small-span sub-stream')
     parser.add_argument('--tune', action='store_true', help='windows: run the autotuner first')
     parser.add_argument('--plain-windows', type=int, default=64,
                         help='windows: how many windows the plain per-window loop is timed and checked on')

@@ -110,6 +110,8 @@ typedef struct pc_stats {
     uint64_t launches;         /* kernels launched by the call */
     uint64_t reserved[5];      /* [0..3]: bitset filters, block words, threads and cheap-tier
                                   filters the call used; [4]: 1 when a recorded graph ran */
+    uint64_t h2d_bytes;        /* bytes the call copied from the host to the device */
+    uint64_t d2h_bytes;        /* bytes the call copied from the device to the host */
 } pc_stats;
 
 /*

@@ -260,8 +260,26 @@ def halves(terms: list[list[int]]) -> tuple[list[list[int]], list[list[int]]]:
             [t for i, t in enumerate(terms) if not best & (1 << i)])
 
 
+@lru_cache(maxsize=1)
+def reference_producer() -> ctypes.CDLL | None:
+    """The reference's own window producer, review/focus_window_cpu.cpp compiled into
+    oracle/_ref by the Makefile (None where it was not built)."""
+    path = REF_DIR / 'focus_window.so'
+    if not path.exists():
+        return None
+    so = ctypes.CDLL(str(path))
+    u64 = ctypes.c_uint64
+    so.focus_window.argtypes = [_U64P, u64, _U64P, u64, u64, u64, u64, u64, ctypes.c_void_p, u64, ctypes.POINTER(u64)]
+    so.focus_window.restype = ctypes.c_int
+    return so
+
+
 class OracleFocus:
-    """Sorted half sums C and D of one focus and the window query over them."""
+    """Sorted half sums C and D of one focus and the window query over them.  ``producer`` is
+    'port' (the C restatement in sieve.c) or 'reference' (the reference's focus_window_cpu.cpp from
+    oracle/_ref, one within-period call per period, then the same sort)."""
+
+    producer = 'port'
 
     def __init__(self, geometry: Geometry, which: str) -> None:
         self.M = geometry.A if which == 'A' else geometry.B
@@ -272,9 +290,43 @@ class OracleFocus:
         lib().oc_sort_u64(self.D, len(self.D))
         self.count = len(self.C) * len(self.D)
 
+    def _reference_window(self, low: int, high: int, cap: int) -> np.ndarray:
+        so = reference_producer()
+        if so is None:
+            raise RuntimeError('oracle/_ref/focus_window.so is not built')
+        if high == low:
+            return np.zeros(0, dtype=np.uint64)
+        p0, p1 = low // self.M, (high - 1) // self.M
+        if p1 - p0 + 1 > 4096:
+            raise OverflowError('oracle window overflow')
+        size = min(cap, 2 * self.count * (high - low) // self.M + 4096)
+        out = np.zeros(max(1, size), dtype=np.uint64)
+        written = 0
+        count = ctypes.c_uint64()
+        for period in range(p0, p1 + 1):
+            base = period * self.M
+            a, b = max(low, base) - base, min(high - base, self.M)
+            while True:
+                view = out[written:]
+                rc = so.focus_window(self.C, len(self.C), self.D, len(self.D), self.M, a, b, base,
+                                     view.ctypes.data, len(view), ctypes.byref(count))
+                if rc != 1:
+                    break
+                if len(out) >= cap:
+                    raise OverflowError('oracle window overflow')
+                out = np.concatenate([out, np.zeros(min(cap, 4 * len(out)) - len(out), dtype=np.uint64)])
+            if rc:
+                raise ValueError('reference window producer rejected the window')
+            written += count.value
+        result = out[:written].copy()
+        lib().oc_sort_u64(result, len(result))
+        return result
+
     def window(self, low: int, high: int, cap: int = 10**6) -> np.ndarray:
         if not 0 <= low <= high < 1 << 64:
             raise ValueError('invalid window')
+        if self.producer == 'reference':
+            return self._reference_window(low, high, cap)
         size = min(cap, 2 * self.count * (high - low) // self.M + 4096)
         while True:
             out = np.zeros(max(1, size), dtype=np.uint64)

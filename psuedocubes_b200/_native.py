@@ -41,11 +41,13 @@ class Tuning(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [('kernel_ms', ctypes.c_double), ('bounds_ms', ctypes.c_double), ('window_ms', ctypes.c_double),
                 ('total_ms', ctypes.c_double), ('work_items', ctypes.c_uint64), ('outputs', ctypes.c_uint64),
-                ('launches', ctypes.c_uint64), ('reserved', ctypes.c_uint64 * 5)]
+                ('launches', ctypes.c_uint64), ('reserved', ctypes.c_uint64 * 5), ('h2d_bytes', ctypes.c_uint64),
+                ('d2h_bytes', ctypes.c_uint64)]
 
     def as_dict(self) -> dict[str, Any]:
         return dict(kernel_ms=self.kernel_ms, bounds_ms=self.bounds_ms, window_ms=self.window_ms,
                     total_ms=self.total_ms, outputs=int(self.outputs), launches=int(self.launches),
+                    h2d_bytes=int(self.h2d_bytes), d2h_bytes=int(self.d2h_bytes),
                     deep_survivors=int(self.work_items), bitset_filters=int(self.reserved[0]),
                     block_words=int(self.reserved[1]), threads=int(self.reserved[2]),
                     cheap_filters=int(self.reserved[3]), graph=bool(self.reserved[4]))

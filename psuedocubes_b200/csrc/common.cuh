@@ -20,6 +20,7 @@ struct pc_ctx {
     cudaEvent_t ev[8] = {};
     cudaEvent_t marks[8] = {};
     uint64_t cap = 0, in_use = 0, peak = 0;
+    uint64_t h2d = 0, d2h = 0;       // bytes the library has copied to and from the host
     int sm_count = 0, cc_major = 0, cc_minor = 0;
     char name[256] = {};
     std::string err;
@@ -41,6 +42,13 @@ void pc_release(pc_ctx *ctx, void *ptr, uint64_t bytes);
         cudaError_t e_ = (call);                                              \
         if (e_ != cudaSuccess) return pc_cuda_fail((ctx), e_, #call);         \
     } while (0)
+
+// An asynchronous copy on the context's stream, counted in ctx->h2d / ctx->d2h.
+inline cudaError_t pc_copy(pc_ctx *ctx, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+    if (kind == cudaMemcpyHostToDevice) ctx->h2d += bytes;
+    else if (kind == cudaMemcpyDeviceToHost) ctx->d2h += bytes;
+    return cudaMemcpyAsync(dst, src, bytes, kind, ctx->stream);
+}
 
 inline int pc_cuda_status(pc_ctx *ctx, cudaError_t e, const char *what) {
     return e == cudaSuccess ? PC_OK : pc_cuda_fail(ctx, e, what);

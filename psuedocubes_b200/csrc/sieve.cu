@@ -1019,10 +1019,10 @@ extern "C" int pc_filters_create(pc_ctx *ctx, uint64_t A, uint64_t B, const uint
         pc_filters_free(ctx, f);
         return rc;
     }
-    cudaMemcpyAsync(f->d_fc, fc.data(), f->fc_bytes, cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemcpyAsync(f->d_fcs, f->fcs.data(), f->fcs_bytes, cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemcpyAsync(f->d_bits, bits.data(), f->bits_bytes, cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemcpyAsync(f->d_pat, pat.data(), f->pat_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    pc_copy(ctx, f->d_fc, fc.data(), f->fc_bytes, cudaMemcpyHostToDevice);
+    pc_copy(ctx, f->d_fcs, f->fcs.data(), f->fcs_bytes, cudaMemcpyHostToDevice);
+    pc_copy(ctx, f->d_bits, bits.data(), f->bits_bytes, cudaMemcpyHostToDevice);
+    pc_copy(ctx, f->d_pat, pat.data(), f->pat_bytes, cudaMemcpyHostToDevice);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
         pc_filters_free(ctx, f);
@@ -1213,11 +1213,10 @@ int engine_prepare(Engine &E, const pc_tuning *tuning, Scratch &hold) {
     if (!rc) rc = hold.get(&E.d_item_next, 1);
     if (!rc) rc = engine_deep_alloc(E, E.deep_cap);
     if (rc) return rc;
-    cudaStream_t st = ctx->stream;
-    PC_CHECK(ctx, cudaMemcpyAsync(E.d_seg, E.segs.data(), E.segs.size() * sizeof(SegDev), cudaMemcpyHostToDevice, st));
-    PC_CHECK(ctx, cudaMemcpyAsync(E.d_fam, E.famdev.data(), E.famdev.size() * sizeof(FamDev), cudaMemcpyHostToDevice, st));
+    PC_CHECK(ctx, pc_copy(ctx, E.d_seg, E.segs.data(), E.segs.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
+    PC_CHECK(ctx, pc_copy(ctx, E.d_fam, E.famdev.data(), E.famdev.size() * sizeof(FamDev), cudaMemcpyHostToDevice));
     if (E.ntiles)
-        PC_CHECK(ctx, cudaMemcpyAsync(E.d_tile_seg, E.tile_seg.data(), E.ntiles * 4, cudaMemcpyHostToDevice, st));
+        PC_CHECK(ctx, pc_copy(ctx, E.d_tile_seg, E.tile_seg.data(), E.ntiles * 4, cudaMemcpyHostToDevice));
     return PC_OK;
 }
 
@@ -1342,8 +1341,7 @@ int engine_eager(Engine &E, int *launches) {
         E.deep_max = 0;
         if (E.nu && E.nv) {
             std::vector<uint32_t> deep_counts(E.grid);
-            PC_CHECK(ctx, cudaMemcpyAsync(deep_counts.data(), E.d_deep_count, (uint64_t)E.grid * 4, cudaMemcpyDeviceToHost,
-                                          ctx->stream));
+            PC_CHECK(ctx, pc_copy(ctx, deep_counts.data(), E.d_deep_count, (uint64_t)E.grid * 4, cudaMemcpyDeviceToHost));
             PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
             for (uint32_t c : deep_counts) E.deep_max = std::max(E.deep_max, c);
             if (E.deep_max > E.deep_cap) {
@@ -1373,17 +1371,17 @@ int engine_collect(Engine &E, uint64_t *counts, uint64_t *geometry, uint64_t *ou
     pc_ctx *ctx = E.ctx;
     cudaStream_t st = ctx->stream;
     unsigned long long nout[2] = {0, 0};
-    PC_CHECK(ctx, cudaMemcpyAsync(nout, E.d_nout, 16, cudaMemcpyDeviceToHost, st));
+    PC_CHECK(ctx, pc_copy(ctx, nout, E.d_nout, 16, cudaMemcpyDeviceToHost));
     if (E.ntiles) {
-        PC_CHECK(ctx, cudaMemcpyAsync(counts, E.d_counts, E.ntiles * E.stride * 8, cudaMemcpyDeviceToHost, st));
-        PC_CHECK(ctx, cudaMemcpyAsync(geometry, E.d_geo, 2 * E.ntiles * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, pc_copy(ctx, counts, E.d_counts, E.ntiles * E.stride * 8, cudaMemcpyDeviceToHost));
+        PC_CHECK(ctx, pc_copy(ctx, geometry, E.d_geo, 2 * E.ntiles * 8, cudaMemcpyDeviceToHost));
     }
     PC_CHECK(ctx, cudaStreamSynchronize(st));
     *n_out = nout[0];
     int rc = engine_check(E, nout, counts);
     if (rc) return rc;
     if (nout[0]) {
-        PC_CHECK(ctx, cudaMemcpyAsync(out, E.d_out, 2 * nout[0] * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, pc_copy(ctx, out, E.d_out, 2 * nout[0] * 8, cudaMemcpyDeviceToHost));
         PC_CHECK(ctx, cudaStreamSynchronize(st));
     }
     return PC_OK;
@@ -1447,6 +1445,7 @@ extern "C" int pc_run_batch(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t
     if (stats) memset(stats, 0, sizeof(*stats));
     *n_out = 0;
     auto t0 = std::chrono::steady_clock::now();
+    const uint64_t h2d0 = ctx->h2d, d2h0 = ctx->d2h;
     Engine E;
     E.ctx = ctx;
     E.us = us->d + u_off;
@@ -1465,7 +1464,11 @@ extern "C" int pc_run_batch(pc_ctx *ctx, const pc_filters *f, const pc_tuning *t
     if (!rc) rc = engine_eager(E, &launches);
     if (!rc) rc = engine_collect(E, counts, geometry, out, n_out);
     if (!rc || rc == PC_OVERFLOW || rc == PC_ARITHMETIC) engine_stats(E, stats, launches, *n_out);
-    if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) {
+        stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        stats->h2d_bytes = ctx->h2d - h2d0;
+        stats->d2h_bytes = ctx->d2h - d2h0;
+    }
     return rc;
 }
 
@@ -1477,6 +1480,7 @@ extern "C" int pc_run_lease(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb,
     if (stats) memset(stats, 0, sizeof(*stats));
     *n_out = 0;
     auto t0 = std::chrono::steady_clock::now();
+    const uint64_t h2d0 = ctx->h2d, d2h0 = ctx->d2h;
     typedef unsigned __int128 w128;
     const w128 lo = (w128)lo1 << 64 | lo0, hi = (w128)hi1 << 64 | hi0;
     const w128 ulo = (lo + (w128)first * f->A) / f->B + 1, uhi = (hi + (w128)(end - 1) * f->A) / f->B + 1;
@@ -1515,7 +1519,11 @@ extern "C" int pc_run_lease(pc_ctx *ctx, const pc_focus *fa, const pc_focus *fb,
         engine_stats(E, stats, launches, *n_out);
         if (stats) stats->window_ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
     }
-    if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) {
+        stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        stats->h2d_bytes = ctx->h2d - h2d0;
+        stats->d2h_bytes = ctx->d2h - d2h0;
+    }
     return rc;
 }
 
@@ -1577,7 +1585,7 @@ extern "C" int pc_run_plain(pc_ctx *ctx, const pc_filters *f, const pc_buf *us, 
         PC_LAUNCHED(ctx, "plain match");
     }
     PC_CHECK(ctx, cudaEventRecord(ctx->ev[7], st));
-    PC_CHECK(ctx, cudaMemcpyAsync(counts, d_counts, (ng + 3) * 8, cudaMemcpyDeviceToHost, st));
+    PC_CHECK(ctx, pc_copy(ctx, counts, d_counts, (ng + 3) * 8, cudaMemcpyDeviceToHost));
     PC_CHECK(ctx, cudaStreamSynchronize(st));
     uint64_t n = counts[ng + 1];
     if (stats) {
@@ -1587,7 +1595,7 @@ extern "C" int pc_run_plain(pc_ctx *ctx, const pc_filters *f, const pc_buf *us, 
     }
     uint64_t copy = std::min(n, out_cap);
     if (copy) {
-        PC_CHECK(ctx, cudaMemcpyAsync(out, d_out, 2 * copy * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, pc_copy(ctx, out, d_out, 2 * copy * 8, cudaMemcpyDeviceToHost));
         PC_CHECK(ctx, cudaStreamSynchronize(st));
     }
     return PC_OK;
@@ -1614,6 +1622,7 @@ struct pc_multi {
     std::vector<uint64_t> counts, geometry, out;
     uint64_t n_out = 0;
     int launches = 0;
+    uint64_t graph_d2h = 0;          // bytes the recorded graph copies to the host per replay
     bool ran = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1774,16 +1783,16 @@ int multi_capture(pc_ctx *ctx, pc_multi *m) {
     if (!rc) rc = winbatch_emit(ctx, m->wb, m->d_lists);
     if (!rc) rc = engine_front(E, false, true, &launches);
     if (!rc) rc = engine_back(E, false, &launches);
-    if (!rc) rc = pc_cuda_status(ctx, cudaMemcpyAsync(m->h_nout, E.d_nout, 16, cudaMemcpyDeviceToHost, st), "capture copy");
+    if (!rc) rc = pc_cuda_status(ctx, pc_copy(ctx, m->h_nout, E.d_nout, 16, cudaMemcpyDeviceToHost), "capture copy");
     if (!rc && E.ntiles) {
-        rc = pc_cuda_status(ctx, cudaMemcpyAsync(m->h_counts, E.d_counts, E.ntiles * E.stride * 8, cudaMemcpyDeviceToHost, st),
+        rc = pc_cuda_status(ctx, pc_copy(ctx, m->h_counts, E.d_counts, E.ntiles * E.stride * 8, cudaMemcpyDeviceToHost),
                             "capture copy");
         if (!rc)
-            rc = pc_cuda_status(ctx, cudaMemcpyAsync(m->h_geo, E.d_geo, 2 * E.ntiles * 8, cudaMemcpyDeviceToHost, st),
+            rc = pc_cuda_status(ctx, pc_copy(ctx, m->h_geo, E.d_geo, 2 * E.ntiles * 8, cudaMemcpyDeviceToHost),
                                 "capture copy");
     }
     if (!rc)
-        rc = pc_cuda_status(ctx, cudaMemcpyAsync(m->h_deep, E.d_deep_count, (uint64_t)E.grid * 4, cudaMemcpyDeviceToHost, st),
+        rc = pc_cuda_status(ctx, pc_copy(ctx, m->h_deep, E.d_deep_count, (uint64_t)E.grid * 4, cudaMemcpyDeviceToHost),
                             "capture copy");
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &g);       // always leave capture mode
@@ -1796,6 +1805,9 @@ int multi_capture(pc_ctx *ctx, pc_multi *m) {
     m->graph = g;
     PC_CHECK(ctx, cudaGraphInstantiate(&m->exec, g, 0));
     m->launches = launches + 5;
+    // the copies recorded into the graph run at every replay, not at capture
+    m->graph_d2h = 16 + (E.ntiles ? E.ntiles * E.stride * 8 + 2 * E.ntiles * 8 : 0) + (uint64_t)E.grid * 4;
+    ctx->d2h -= m->graph_d2h;
     return PC_OK;
 }
 
@@ -1806,6 +1818,7 @@ int multi_replay(pc_ctx *ctx, pc_multi *m, pc_stats *stats) {
     if (rc) return rc;
     PC_CHECK(ctx, cudaEventRecord(ctx->ev[0], st));
     PC_CHECK(ctx, cudaGraphLaunch(m->exec, st));
+    ctx->d2h += m->graph_d2h;
     PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], st));
     PC_CHECK(ctx, cudaStreamSynchronize(st));
     for (int b = 0; b < E.grid; ++b)
@@ -1816,7 +1829,7 @@ int multi_replay(pc_ctx *ctx, pc_multi *m, pc_stats *stats) {
     m->n_out = nout[0];
     rc = engine_check(E, nout, m->counts.data());
     if (!rc && nout[0]) {
-        PC_CHECK(ctx, cudaMemcpyAsync(m->out.data(), E.d_out, 2 * nout[0] * 8, cudaMemcpyDeviceToHost, st));
+        PC_CHECK(ctx, pc_copy(ctx, m->out.data(), E.d_out, 2 * nout[0] * 8, cudaMemcpyDeviceToHost));
         PC_CHECK(ctx, cudaStreamSynchronize(st));
     }
     if (stats) {
@@ -1839,6 +1852,7 @@ extern "C" int pc_multi_run(pc_ctx *ctx, pc_multi *m, uint32_t flags, pc_stats *
     if (!m) return pc_fail(ctx, PC_INVALID, "no window batch");
     if (stats) memset(stats, 0, sizeof(*stats));
     auto t0 = std::chrono::steady_clock::now();
+    const uint64_t h2d0 = ctx->h2d, d2h0 = ctx->d2h;
     int rc = PC_OK;
     if (!(flags & PC_RUN_GRAPH) || !m->ran) {
         rc = multi_eager(ctx, m, stats);
@@ -1848,7 +1862,11 @@ extern "C" int pc_multi_run(pc_ctx *ctx, pc_multi *m, uint32_t flags, pc_stats *
         if (!m->exec) rc = multi_capture(ctx, m);
         if (!rc) rc = multi_replay(ctx, m, stats);
     }
-    if (stats) stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) {
+        stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        stats->h2d_bytes = ctx->h2d - h2d0;
+        stats->d2h_bytes = ctx->d2h - d2h0;
+    }
     return rc;
 }
 

@@ -360,7 +360,7 @@ extern "C" int pc_focus_create(pc_ctx *ctx, uint64_t M, uint32_t nrings, const u
         delete f;
         return rc;
     }
-    if (!pat.empty()) cudaMemcpyAsync(d_pat, pat.data(), pat.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (!pat.empty()) pc_copy(ctx, d_pat, pat.data(), pat.size() * 4, cudaMemcpyHostToDevice);
     uint64_t nwords = (f->M1 + 31) / 32;
     uint64_t nthreads = (nwords + SIEVE_WORDS - 1) / SIEVE_WORDS;
     uint64_t *d_cnt, *d_off, *d_total;
@@ -375,7 +375,7 @@ extern "C" int pc_focus_create(pc_ctx *ctx, uint64_t M, uint32_t nrings, const u
     k_sieve<<<grid, WT, 0, ctx->stream>>>(sr, d_pat, f->M1, nwords, d_cnt, nullptr, nullptr);
     rc = pc_exclusive_scan_u64(ctx, d_cnt, d_off, nthreads, d_total);
     uint64_t total = 0;
-    if (!rc && cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream) == cudaSuccess &&
+    if (!rc && pc_copy(ctx, &total, d_total, 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
         cudaStreamSynchronize(ctx->stream) == cudaSuccess) {
     } else if (!rc) {
         rc = pc_cuda_fail(ctx, cudaGetLastError(), "wheel count");
@@ -431,7 +431,7 @@ extern "C" int pc_focus_create(pc_ctx *ctx, uint64_t M, uint32_t nrings, const u
         uint32_t *d_rp;
         rc = s.get(&d_rp, words.size());
         if (rc) break;
-        cudaMemcpyAsync(d_rp, words.data(), words.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+        pc_copy(ctx, d_rp, words.data(), words.size() * 4, cudaMemcpyHostToDevice);
         uint64_t threads = f->words1 * 32;
         k_wheel_rows<<<(unsigned)((threads + WT - 1) / WT), WT, 0, ctx->stream>>>(
             f->W1, f->count1, f->words1, d_rp, r.q, make_modq(r.q), f->rows + (uint64_t)f->t_row0[t] * f->words1);
@@ -443,7 +443,7 @@ extern "C" int pc_focus_create(pc_ctx *ctx, uint64_t M, uint32_t nrings, const u
     }
     if (!rc) {
         f->W1_host.resize(f->count1);
-        cudaError_t e = cudaMemcpyAsync(f->W1_host.data(), f->W1, f->count1 * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaError_t e = pc_copy(ctx, f->W1_host.data(), f->W1, f->count1 * 8, cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = pc_cuda_fail(ctx, e, "wheel download");
     }
@@ -592,14 +592,14 @@ int winbatch_plan(pc_ctx *ctx, Scratch &hold, const pc_focus *const *focus, cons
     if (rc) return rc;
     wb.d_desc = d_desc;
     wb.d_foci = d_foci;
-    PC_CHECK(ctx, cudaMemcpyAsync(d_desc, desc.data(), n * sizeof(WinDesc), cudaMemcpyHostToDevice, ctx->stream));
-    PC_CHECK(ctx, cudaMemcpyAsync(d_foci, foci.data(), foci.size() * sizeof(FocusDev), cudaMemcpyHostToDevice, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, d_desc, desc.data(), n * sizeof(WinDesc), cudaMemcpyHostToDevice));
+    PC_CHECK(ctx, pc_copy(ctx, d_foci, foci.data(), foci.size() * sizeof(FocusDev), cudaMemcpyHostToDevice));
     rc = winbatch_count(ctx, wb);
     if (rc) return rc;
     k_window_totals<<<(n + 255) / 256, 256, 0, ctx->stream>>>(d_desc, n, wb.d_off, wb.d_tot);
     PC_LAUNCHED(ctx, "window totals");
     wb.total.assign(n, 0);
-    PC_CHECK(ctx, cudaMemcpyAsync(wb.total.data(), wb.d_tot, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, wb.total.data(), wb.d_tot, n * 8, cudaMemcpyDeviceToHost));
     PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
     wb.base.assign(n, 0);
     for (uint32_t i = 0; i < n; ++i) {
@@ -608,7 +608,7 @@ int winbatch_plan(pc_ctx *ctx, Scratch &hold, const pc_focus *const *focus, cons
         wb.base[i] = (wb.out_len + pd - 1) / pd * pd;
         wb.out_len = wb.base[i] + wb.total[i];
     }
-    PC_CHECK(ctx, cudaMemcpyAsync(wb.d_base, wb.base.data(), n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, wb.d_base, wb.base.data(), n * 8, cudaMemcpyHostToDevice));
     PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));   // the host vectors above go out of scope
     if (launches) *launches += 4;
     return PC_OK;

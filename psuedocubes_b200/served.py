@@ -295,7 +295,7 @@ class ServedLoop:
             tile = (r2[:, 1] >> np.uint64(32)) + np.uint64(half)
             r2[:, 1] = (r2[:, 1] & np.uint64(0xFFFFFFFF)) | (tile << np.uint64(32))
         stats = {k: s1.get(k, 0) + s2.get(k, 0) for k in ('kernel_ms', 'total_ms', 'window_ms', 'bounds_ms',
-                                                        'u_entries', 'v_entries')}
+                                                        'u_entries', 'v_entries', 'launches', 'h2d_bytes', 'd2h_bytes')}
         return np.vstack([pad(c1), pad(c2)]), np.vstack([r1, r2]), stats, n1 + n2
 
     def run(self, requests: list[Request], realtime: bool = True, time_limit: float = float('inf'),
@@ -378,7 +378,8 @@ class ServedLoop:
                 w.outstanding -= 1
             self.steps.append(dict(windows=len(step), positions=int(counts[:, 0].sum()),
                                    **{k: stats.get(k, 0) for k in ('kernel_ms', 'total_ms', 'window_ms', 'bounds_ms',
-                                                                   'u_entries', 'v_entries')}))
+                                                                   'u_entries', 'v_entries', 'launches', 'h2d_bytes',
+                                                                   'd2h_bytes')}))
             for w in [w for w in active if not w.pending and not w.outstanding]:
                 active.remove(w)
                 self.reserved -= w.reserved
@@ -490,15 +491,26 @@ def plain_loop(runtime: Runtime, requests: list[Request], time_limit: float = fl
 
 
 def latency_summary(run: dict[str, Any], requests: list[Request]) -> dict[str, Any]:
-    """p50/p99 over all requests; an unfinished request counts with the run's end as its latency
-    (a lower bound)."""
+    """p50/p99 over all requests; an unfinished request counts with the run's end as its latency,
+    so with any unfinished request (``censored``) the percentiles are lower bounds."""
     lat = [r['latency'] for r in run['results'].values()]
-    lat += [run['seconds'] - req.arrival for req in requests if req.id in set(run['unfinished'])]
+    unfinished = set(run['unfinished'])
+    lat += [run['seconds'] - req.arrival for req in requests if req.id in unfinished]
     lat.sort()
     pick = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
     return dict(p50=pick(0.5), p99=pick(0.99), requests=len(requests), completed=len(run['results']),
+                censored=bool(unfinished),
                 positions_per_second=run['positions'] / run['seconds'] if run['seconds'] else None)
 
 
+def rescaled(requests: list[Request], rate: float) -> list[Request]:
+    """The same requests with their arrival gaps scaled to a mean rate of ``rate`` per second."""
+    if not requests:
+        return []
+    mean_gap = requests[-1].arrival / max(1, len(requests) - 1) if len(requests) > 1 else 1.0 / rate
+    scale = (1.0 / rate) / mean_gap if mean_gap > 0 else 1.0
+    return [Request(r.id, r.p, r.lo, r.hi, r.arrival * scale) for r in requests]
+
+
 __all__ = ['Request', 'Plan', 'plan_request', 'split_plan', 'poisson_requests', 'request_windows', 'ServedLoop',
-           'plain_request', 'plain_loop', 'latency_summary', 'A_RINGS', 'B_RINGS', 'SERVED_PRIMES']
+           'plain_request', 'plain_loop', 'latency_summary', 'rescaled', 'A_RINGS', 'B_RINGS', 'SERVED_PRIMES']

@@ -11,6 +11,8 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = ROOT / 'tests' / 'golden'
+#: the reference project's tree; the CPU tests that import its unchanged host code skip without it
+REFERENCE = Path(os.environ.get('PSUEDOCUBES_REFERENCE', '/root/reference'))
 sys.path.insert(0, str(ROOT))
 
 

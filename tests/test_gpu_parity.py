@@ -357,3 +357,23 @@ def test_bench_leases_match_oracle_whole(runtime, p619, focuses619, oracle, orac
                 'subtiles_executed'):
         assert got[key] == want[key], key
     assert [h['n'] for h in got['cpu_confirmed_hits']] == [h['n'] for h in want['cpu_confirmed_hits']]
+
+
+def test_calls_report_the_bytes_they_copy(runtime, p619, focuses619):
+    """pc_stats counts the library's own host transfers: a lease uploads its window, segment and
+    subtile descriptors and brings back counters, envelope sizes, records and scalars."""
+    import ctypes
+    from psuedocubes_b200.gpu import MASK
+    fa, fb = focuses619
+    m = MaskedMatcher(runtime, p619)
+    first, end = 658625401600000000, 658625401600000000 + 2 * BATCH_WIDTH
+    nt, ng = 128, len(m.filter_groups)
+    counts, geometry = np.zeros(nt * (ng + 3), dtype=np.uint64), np.zeros(2 * nt, dtype=np.uint64)
+    records, n_out, stats = np.zeros(2 * 1024, dtype=np.uint64), ctypes.c_uint64(), N.Stats()
+    c = p619
+    runtime.call(runtime.lib.pc_run_lease(runtime.ctx, fa.handle, fb.handle, m.filters.handle, ctypes.byref(m.tuning),
+                                          first, end, 100_000_000, c.lo & MASK, c.lo >> 64, c.hi & MASK, c.hi >> 64,
+                                          counts, geometry, records, 1024, ctypes.byref(n_out), ctypes.byref(stats)))
+    s = stats.as_dict()
+    assert nt * 4 <= s['h2d_bytes'] < 1 << 20                        # the subtile map and descriptors
+    assert s['d2h_bytes'] >= counts.nbytes + geometry.nbytes + 16 + 16 * n_out.value
