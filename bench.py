@@ -344,15 +344,33 @@ def run_windows(args) -> None:
     batch.close()
     # end to end through the public API: plan (descriptors to the device), eager run, results with
     # host verification of every window
-    e2e_times = []
+    e2e_times, phases = [], []
     rows = None
+    c0 = runtime.copies()
     for _ in range(max(1, args.e2e_steps)):
         t0 = time.perf_counter()
         b = engine.plan(windows, settings['width'], tuning, output_cap=1 << 16)
+        t1 = time.perf_counter()
         b.run()
+        t2 = time.perf_counter()
         rows = b.results()
         b.close()
-        e2e_times.append(time.perf_counter() - t0)
+        t3 = time.perf_counter()
+        e2e_times.append(t3 - t0)
+        phases.append((t1 - t0, t2 - t1, t3 - t2))
+    c1 = runtime.copies()
+    e2e_steps = max(1, args.e2e_steps)
+    e2e_h2d, e2e_d2h = (c1[0] - c0[0]) // e2e_steps, (c1[1] - c0[1]) // e2e_steps
+    # the recorded graph replayed on its resident windows, with the results on the host each step
+    replay = engine.plan(windows, settings['width'], tuning, output_cap=1 << 16)
+    replay.run(graph=True)
+    replay_times = []
+    for _ in range(max(1, args.e2e_steps)):
+        t0 = time.perf_counter()
+        replay.run(graph=True)
+        replay.results()
+        replay_times.append(time.perf_counter() - t0)
+    replay.close()
     # the plain per-window tile loop (Matcher.tile over 1e8-v tiles) on a sample, checked per window
     sample = windows[:args.plain_windows]
     mismatches, plain_positions = 0, 0
@@ -373,8 +391,7 @@ def run_windows(args) -> None:
         peak = runtime.sm_count * 4 * 32 * sm_mhz * 1e6 / 1e12
         mean_graph_ms = sum(graph_ms) / len(graph_ms)
         achieved = OPS_PER_POSITION * positions / (mean_graph_ms / 1000) / 1e12
-        d2h = counts.nbytes + geometry.nbytes + records.nbytes + 16
-        h2d = 64 * len(windows)
+        plan_s, run_s, results_s = (statistics.median(p[k] for p in phases) for k in range(3))
         line = dict(metric=WINDOWS_METRIC, value=positions * world * args.steps / seconds, unit=UNIT, n_gpus=world,
                     steps=args.steps, warmup=args.warmup, ms_per_step=1000 * seconds / args.steps,
                     higher_is_better=True, scaling='weak', vs_baseline=None, dtype='u64', data='synthetic',
@@ -389,8 +406,12 @@ def run_windows(args) -> None:
                                   traffic_unit='bytes per replay (lease ncu capture, scaled by positions)',
                                   kernel='whole graph (windows, bounds, k_match, k_deep): a lower bound for k_match',
                                   ops_per_position=OPS_PER_POSITION),
-                    e2e=dict(value=positions * world / statistics.median(e2e_times), unit=UNIT, h2d_bytes_per_step=h2d,
-                             d2h_bytes_per_step=int(d2h), api='BatchedEngine.plan + WindowBatch.run + results'),
+                    e2e=dict(value=positions * world / statistics.median(e2e_times), unit=UNIT,
+                             h2d_bytes_per_step=int(e2e_h2d), d2h_bytes_per_step=int(e2e_d2h),
+                             api='BatchedEngine.plan + WindowBatch.run + results',
+                             ms=dict(plan=1000 * plan_s, run=1000 * run_s, results=1000 * results_s)),
+                    replay_e2e=dict(value=positions * world / statistics.median(replay_times), unit=UNIT,
+                                    api='WindowBatch.run(graph=True) + results on a planned batch'),
                     eager=dict(ms=eager['total_ms'], kernel_ms=eager['kernel_ms'], window_ms=eager['window_ms']),
                     plain_path=dict(value=plain_positions / plain_seconds, unit=UNIT, windows=len(sample),
                                     seconds=plain_seconds, mismatches=mismatches,

@@ -42,6 +42,10 @@ const char *pc_last_error(const pc_ctx *ctx);
 int pc_init(int device, uint64_t mem_cap, double fraction, pc_ctx **out);
 int pc_free(pc_ctx *ctx);
 int pc_mem_info(const pc_ctx *ctx, uint64_t *in_use, uint64_t *peak, uint64_t *cap);
+/* Bytes the library has copied from the host to the device and back on this context so far
+ * (the reference's Runtime keeps no such count; a caller takes differences around any sequence
+ * of calls, e.g. a window plan and its run). */
+int pc_copy_info(const pc_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
 int pc_device_info(const pc_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor, char *name, int name_len);
 
 /* Page-locked host memory for result buffers (counts, geometry, outputs): device-to-host copies

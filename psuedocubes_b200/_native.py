@@ -22,7 +22,8 @@ LIB_PATH = LIB_DIR / 'libpcube.so'
 PC_OK, PC_OVERFLOW, PC_INVALID, PC_ARITHMETIC, PC_TIMEOUT, PC_NOMEM, PC_CUDA = range(7)
 
 #: Every symbol include/pcube.h declares.
-SYMBOLS = ('pc_version', 'pc_device_count', 'pc_last_error', 'pc_init', 'pc_free', 'pc_mem_info', 'pc_host_alloc', 'pc_host_free',
+SYMBOLS = ('pc_version', 'pc_device_count', 'pc_last_error', 'pc_init', 'pc_free', 'pc_mem_info', 'pc_copy_info',
+           'pc_host_alloc', 'pc_host_free',
            'pc_device_info', 'pc_sync', 'pc_mark', 'pc_elapsed', 'pc_buf_upload', 'pc_buf_download', 'pc_buf_size', 'pc_buf_free',
            'pc_buf_searchsorted', 'pc_focus_create', 'pc_focus_free', 'pc_focus_info', 'pc_focus_window',
            'pc_filters_create', 'pc_filters_free', 'pc_run_batch', 'pc_run_lease', 'pc_run_leases', 'pc_multi_create',
@@ -83,6 +84,7 @@ def lib() -> ctypes.CDLL:
     so.pc_init.argtypes = [ctypes.c_int, _U64, ctypes.c_double, pp]
     so.pc_free.argtypes = [_P]
     so.pc_mem_info.argtypes = [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_U64)]
+    so.pc_copy_info.argtypes = [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]
     so.pc_device_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int]
     so.pc_sync.argtypes = [_P]

@@ -247,14 +247,26 @@ class WindowBatch:
         cuts = np.searchsorted(tile_sorted, np.arange(nt + 1))
         valid = counts[:, 0].tolist()
         emitted_list = emitted.tolist()
-        table = counts.tolist()
         sums = np.add.reduceat(counts, tb[:-1], axis=0).tolist() if nt else [[0] * self.stride] * n
         gu, gv = geometry[:, 0].tolist(), geometry[:, 1].tolist()
+        # group populations as Python lists, one conversion per family over the family's subtiles
+        family_rows: dict[int, list] = {}
+        where: list[tuple[list, int]] = []
+        for f in sorted(set(self._family_of)):
+            members = [i for i in range(n) if self._family_of[i] == f]
+            sel = np.concatenate([np.arange(tb[i], tb[i + 1]) for i in members])
+            family_rows[f] = counts[sel, 1:self.families[f].ng + 1].tolist()
+        offsets = {f: 0 for f in family_rows}
+        for i in range(n):
+            f = self._family_of[i]
+            where.append((family_rows[f], offsets[f]))
+            offsets[f] += int(tb[i + 1] - tb[i])
         out = []
         for i, (w, c) in enumerate(zip(self.windows, self.configs)):
             t0, t1, ng = int(tb[i]), int(tb[i + 1]), int(ngs[i])
             width = self.widths[i]
-            group_rows = [row[1:ng + 1] for row in table[t0:t1]]
+            rows_f, at0 = where[i]
+            group_rows = rows_f[at0:at0 + t1 - t0]
             firsts = range(w.first, w.end, width)
             digests, values = [EMPTY_DIGEST] * (t1 - t0), []
             for t in range(t0, t1):
@@ -269,9 +281,11 @@ class WindowBatch:
                 digests[t - t0] = digest([str(x) for x in tile_values])
                 values.extend(tile_values)
             hits = verify_values(c, values) if values else []
-            scopes = [dict(first=str(f), end=str(min(f + width, w.end)), valid_focused_candidates=v,
-                           group_survivors=g, local_survivors=e, output_sha256=d)
-                      for f, v, g, e, d in zip(firsts, valid[t0:t1], group_rows, emitted_list[t0:t1], digests)]
+            starts = list(map(str, firsts))
+            ends = starts[1:] + [str(w.end)]
+            scopes = [{'first': a, 'end': b, 'valid_focused_candidates': v, 'group_survivors': g, 'local_survivors': e,
+                       'output_sha256': d}
+                      for a, b, v, g, e, d in zip(starts, ends, valid[t0:t1], group_rows, emitted_list[t0:t1], digests)]
             us, vs = gu[t0:t1], gv[t0:t1]
             row = dict(status='PASS', host_verified=True, focus_u=int(self.sizes[2 * i]),
                        focus_v=int(self.sizes[2 * i + 1]), cartesian_opportunities=sum(a * b for a, b in zip(us, vs)),

@@ -169,7 +169,7 @@ extern "C" int pc_cube_roots(pc_ctx *ctx, uint64_t first, uint64_t last, uint32_
     const uint64_t warps = ROOT_THREADS / 32;
     const unsigned grid = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((nchunks + warps - 1) / warps, (uint64_t)ctx->sm_count * std::max(1, per_sm)));
-    PC_CHECK(ctx, cudaMemcpyAsync(d_tables, host.data(), smem, cudaMemcpyHostToDevice, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, d_tables, host.data(), smem, cudaMemcpyHostToDevice));
     PC_CHECK(ctx, cudaMemsetAsync(d_total, 0, 8, ctx->stream));
     auto elapsed = [&](float &ms) { return cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]); };
     if (!roots) {
@@ -179,7 +179,7 @@ extern "C" int pc_cube_roots(pc_ctx *ctx, uint64_t first, uint64_t last, uint32_
         PC_LAUNCHED(ctx, "cube roots count");
         PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
         unsigned long long total = 0;
-        PC_CHECK(ctx, cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PC_CHECK(ctx, pc_copy(ctx, &total, d_total, 8, cudaMemcpyDeviceToHost));
         PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
         float ms = 0;
         PC_CHECK(ctx, elapsed(ms));
@@ -200,7 +200,7 @@ extern "C" int pc_cube_roots(pc_ctx *ctx, uint64_t first, uint64_t last, uint32_
     rc = pc_exclusive_scan_ws(ctx, d_counts, d_offsets, nchunks, d_offsets + nchunks, d_ws);
     if (rc) return rc;
     uint64_t total = 0;
-    PC_CHECK(ctx, cudaMemcpyAsync(&total, d_offsets + nchunks, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, &total, d_offsets + nchunks, 8, cudaMemcpyDeviceToHost));
     PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
     float ms = 0;
     PC_CHECK(ctx, elapsed(ms));
@@ -216,7 +216,7 @@ extern "C" int pc_cube_roots(pc_ctx *ctx, uint64_t first, uint64_t last, uint32_
                                                        nullptr, nullptr, d_offsets, d_out);
     PC_LAUNCHED(ctx, "cube roots emit");
     PC_CHECK(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
-    PC_CHECK(ctx, cudaMemcpyAsync(roots, d_out, total * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, roots, d_out, total * 4, cudaMemcpyDeviceToHost));
     PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
     float emit_ms = 0;
     PC_CHECK(ctx, elapsed(emit_ms));

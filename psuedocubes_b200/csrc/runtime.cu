@@ -128,6 +128,13 @@ extern "C" int pc_mem_info(const pc_ctx *ctx, uint64_t *in_use, uint64_t *peak, 
     return PC_OK;
 }
 
+extern "C" int pc_copy_info(const pc_ctx *ctx, uint64_t *h2d, uint64_t *d2h) {
+    if (!ctx || !h2d || !d2h) return PC_INVALID;
+    *h2d = ctx->h2d;
+    *d2h = ctx->d2h;
+    return PC_OK;
+}
+
 extern "C" int pc_device_info(const pc_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor, char *name, int name_len) {
     *sm_count = ctx->sm_count;
     *cc_major = ctx->cc_major;
@@ -173,7 +180,7 @@ extern "C" int pc_buf_upload(pc_ctx *ctx, const uint64_t *host, uint64_t n, pc_b
         return rc;
     }
     if (n) {
-        cudaError_t e = cudaMemcpyAsync(b->d, host, n * 8, cudaMemcpyHostToDevice, ctx->stream);
+        cudaError_t e = pc_copy(ctx, b->d, host, n * 8, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) {
             pc_release(ctx, b->d, b->bytes);
@@ -188,7 +195,7 @@ extern "C" int pc_buf_upload(pc_ctx *ctx, const uint64_t *host, uint64_t n, pc_b
 extern "C" int pc_buf_download(pc_ctx *ctx, const pc_buf *buf, uint64_t offset, uint64_t n, uint64_t *host) {
     if (offset > buf->n || n > buf->n - offset) return pc_fail(ctx, PC_INVALID, "download out of range");
     if (!n) return PC_OK;
-    PC_CHECK(ctx, cudaMemcpyAsync(host, buf->d + offset, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, host, buf->d + offset, n * 8, cudaMemcpyDeviceToHost));
     PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
     return PC_OK;
 }
@@ -225,10 +232,10 @@ extern "C" int pc_buf_searchsorted(pc_ctx *ctx, const pc_buf *buf, const uint64_
     int rc = s.get(&dq, n);
     if (!rc) rc = s.get(&dp, n);
     if (rc) return rc;
-    PC_CHECK(ctx, cudaMemcpyAsync(dq, queries, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, dq, queries, n * 8, cudaMemcpyHostToDevice));
     k_searchsorted<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(buf->d, buf->n, dq, n, dp);
     PC_LAUNCHED(ctx, "searchsorted");
-    PC_CHECK(ctx, cudaMemcpyAsync(positions, dp, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, positions, dp, n * 8, cudaMemcpyDeviceToHost));
     PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
     return PC_OK;
 }
@@ -353,10 +360,10 @@ extern "C" int pc_selftest_wide(pc_ctx *ctx, const uint64_t *in4, uint64_t *out3
     int rc = s.get(&din, 4 * n);
     if (!rc) rc = s.get(&dout, 3 * n);
     if (rc) return rc;
-    PC_CHECK(ctx, cudaMemcpyAsync(din, in4, 32 * n, cudaMemcpyHostToDevice, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, din, in4, 32 * n, cudaMemcpyHostToDevice));
     k_wide<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(din, dout, n);
     PC_LAUNCHED(ctx, "wide self-test");
-    PC_CHECK(ctx, cudaMemcpyAsync(out3, dout, 24 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    PC_CHECK(ctx, pc_copy(ctx, out3, dout, 24 * n, cudaMemcpyDeviceToHost));
     PC_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
     return PC_OK;
 }

@@ -52,6 +52,12 @@ class Runtime:
         self.lib.pc_mem_info(self.ctx, ctypes.byref(in_use), ctypes.byref(peak), ctypes.byref(cap))
         return in_use.value, peak.value, cap.value
 
+    def copies(self) -> tuple[int, int]:
+        """(host-to-device, device-to-host) bytes the library has copied on this context so far."""
+        h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+        self.call(self.lib.pc_copy_info(self.ctx, ctypes.byref(h2d), ctypes.byref(d2h)))
+        return h2d.value, d2h.value
+
     def check(self) -> None:
         if time.monotonic() >= self.deadline - 3:
             raise TimeoutError('BUDGET_EXHAUSTED')

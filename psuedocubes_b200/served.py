@@ -273,9 +273,12 @@ class ServedLoop:
         """One multi-window launch (one subtile per window).  A step whose outputs overflow the
         output buffer is split in halves and rerun; counters of an overflowed run are complete, but
         its outputs are not, so nothing of it is kept."""
+        before = self.runtime.copies()
         batch = self.engine.plan(windows, None, self.tuning, self.output_cap)
         try:
             stats = dict(batch.run())
+            after = self.runtime.copies()
+            stats.update(h2d_bytes=after[0] - before[0], d2h_bytes=after[1] - before[1])
             stats.update(u_entries=batch.layout['u_entries'], v_entries=batch.layout['v_entries'])
             counts, _, records = batch.raw()
             ngs = [batch.families[batch._family_of[i]].ng for i in range(len(windows))]
