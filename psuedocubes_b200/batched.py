@@ -26,9 +26,10 @@ import json
 import os
 import random
 import time
+from concurrent.futures import Future, ThreadPoolExecutor
 from dataclasses import dataclass, field
 from pathlib import Path
-from typing import Any, Iterable
+from typing import Any, Iterable, Iterator
 
 import numpy as np
 
@@ -125,6 +126,38 @@ class BatchedEngine:
              output_cap: int = 1 << 16) -> 'WindowBatch':
         """Plan a window batch; width None gives every window a single subtile."""
         return WindowBatch(self, windows, width, tuning, output_cap)
+
+    def stream(self, window_sets: Iterable[list[Window]], width: int | None = 100_000_000,
+               tuning: dict[str, int] | None = None, output_cap: int = 1 << 16,
+               graph: bool = False) -> Iterator[list[dict[str, Any]]]:
+        """The results of consecutive window sets, in order.  One device thread plans, runs and
+        copies back set k + 1 while the caller's thread assembles and verifies the results of set
+        k, so the host work overlaps the device work; every library call stays on the device
+        thread.  A consumer that stops early lets the set in flight finish first."""
+        def device(windows: list[Window]) -> tuple['WindowBatch', tuple[np.ndarray, np.ndarray, np.ndarray]]:
+            batch = self.plan(windows, width, tuning, output_cap)
+            try:
+                batch.run(graph=graph)
+                return batch, batch.raw()
+            finally:
+                batch.close()
+
+        pool = ThreadPoolExecutor(1)
+        pending: Future | None = None
+        try:
+            for windows in window_sets:
+                upcoming = pool.submit(device, list(windows))
+                if pending is not None:
+                    batch, raw = pending.result()
+                    pending = None
+                    yield batch.assemble(*raw)
+                pending = upcoming
+            if pending is not None:
+                batch, raw = pending.result()
+                pending = None
+                yield batch.assemble(*raw)
+        finally:
+            pool.shutdown(wait=True)
 
 
 def _tuning(settings: dict[str, int] | None) -> N.Tuning:
@@ -225,9 +258,13 @@ class WindowBatch:
 
     def results(self) -> list[dict[str, Any]]:
         """Per-window results of the last run, host-verified like the reference's tile results
-        (the fields of batch_experiment.batch_result).  Counters of all windows are reduced in a
-        few array passes; only windows that emitted values touch them one by one."""
-        counts, geometry, records = self.raw()
+        (the fields of batch_experiment.batch_result)."""
+        return self.assemble(*self.raw())
+
+    def assemble(self, counts: np.ndarray, geometry: np.ndarray, records: np.ndarray) -> list[dict[str, Any]]:
+        """Per-window results from the raw counters, envelope sizes and output records of a run
+        (host work only).  Counters of all windows are reduced in a few array passes; only
+        windows that emitted values touch them one by one."""
         n, nt = len(self.windows), self.ntiles
         tb = self.tile_base.astype(np.int64)
         ngs = np.array([self.families[self._family_of[i]].ng for i in range(n)], dtype=np.int64)

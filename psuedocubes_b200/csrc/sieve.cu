@@ -332,9 +332,9 @@ __global__ void k_blocks(const VRec *__restrict__ rec, const SegDev *__restrict_
     pieces[b] = vb > va ? vb - va : 0;
 }
 
-// v chunk per work item: fixed, or total pieces / target items, at least min_chunk (two rounds of
-// 32 rows for every warp of a k_match CTA, so a small launch does not leave warps idle) and at
-// most 2^20.
+// v chunk per work item: fixed, or total pieces / target items, at least min_chunk (four rounds of
+// 32 rows for every warp of a k_match CTA, so a small launch keeps every warp busy and pays the
+// per-item set-up over enough rows) and at most 2^20.
 __global__ void k_chunk(const uint64_t *__restrict__ total_pieces, uint64_t fixed_chunk, uint64_t target_items,
                         uint64_t min_chunk, uint64_t *__restrict__ vchunk) {
     uint64_t c = fixed_chunk;
@@ -1288,7 +1288,7 @@ int engine_front(Engine &E, bool events, bool capturing, int *launches) {
     PC_LAUNCHED(ctx, "blocks");
     int rc = pc_exclusive_scan_ws(ctx, E.d_pieces, E.d_tmp, E.nblocks, E.d_tmp + E.nblocks, E.d_ws);
     if (rc) return rc;
-    k_chunk<<<1, 1, 0, st>>>(E.d_tmp + E.nblocks, E.tn.v_chunk, (uint64_t)E.grid * 32, 2 * (uint64_t)E.tn.threads,
+    k_chunk<<<1, 1, 0, st>>>(E.d_tmp + E.nblocks, E.tn.v_chunk, (uint64_t)E.grid * 32, 4 * (uint64_t)E.tn.threads,
                              E.d_vchunk);
     PC_LAUNCHED(ctx, "chunk");
     k_item_counts<<<(unsigned)((E.nblocks + 255) / 256), 256, 0, st>>>(E.d_pieces, E.nblocks, E.d_vchunk, E.d_items);

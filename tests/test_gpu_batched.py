@@ -175,3 +175,21 @@ def test_autotuner_persists_a_choice(runtime, engine, tmp_path):
     assert [r['group_survivors'] for r in batch.results()] == [r['group_survivors'] for r in ref.results()]
     batch.close()
     ref.close()
+
+
+def test_stream_equals_one_set_at_a_time(runtime, engine):
+    """BatchedEngine.stream overlaps the host results of one window set with the device run of
+    the next; every set's results must equal planning and running it alone, in order, and a
+    consumer that stops early leaves the engine usable."""
+    sets = [seeded_windows(12, seed=s, span_exp=(6.0, 9.0)) for s in (1, 2, 3)]
+    want = []
+    for ws in sets:
+        b = engine.plan(ws, width=1 << 24)
+        b.run()
+        want.append(b.results())
+        b.close()
+    assert list(engine.stream(sets, width=1 << 24)) == want
+    gen = engine.stream(sets, width=1 << 24)
+    assert next(gen) == want[0]
+    gen.close()
+    assert list(engine.stream(sets[2:], width=1 << 24, graph=True)) == want[2:]
