@@ -427,7 +427,8 @@ struct MatchSmem {
         fam = cnt + round16(tmax * (ng + 2) * 4);
         seg = fam + round16(sizeof(FamDev));
         misc = seg + round16(sizeof(SegDev));
-        total = misc + 16;                                // deep counter (4 B) and the item grab (8 B at +8)
+        total = misc + 32;   // deep counter (4 B), the item grab (8 B at +8), the item's first subtile and
+                             // its segment's subtile end (8 B each at +16 and +24)
     }
 };
 
@@ -505,6 +506,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     FamDev &F = *(FamDev *)(base + L.fam);
     SegDev &S = *(SegDev *)(base + L.seg);
     uint32_t *deep_ctr = (uint32_t *)(base + L.misc);
+    volatile uint64_t *item_s = (volatile uint64_t *)(base + L.misc + 16);
     const uint32_t cstride = ngmax + 2;
 
     const uint32_t lanes_below = (1u << lane) - 1u;
@@ -580,15 +582,20 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             cur = b;
         }
         for (uint32_t k = threadIdx.x; k < a.tmax * cstride; k += blockDim.x) cnt_s[k] = 0;
+        if (threadIdx.x == 0) {                           // the item's first subtile, once per CTA
+            item_s[0] = S.tile_base + local_tile(a.rec[va].v, S.v_first, S.width, S.ntiles);
+            item_s[1] = (uint64_t)S.tile_base + S.ntiles;
+        }
         __syncthreads();
-        // subtile geometry of the segment stays in shared memory (S): it is read only when a lane's
-        // subtile changes and when a queued survivor needs its subtile recomputed
-        const uint64_t seg_tiles_end = (uint64_t)S.tile_base + S.ntiles;
+        // subtile geometry of the segment and of the item stays in shared memory (S, item_s): it is
+        // read when a lane's subtile changes, once per round for the survivor slots, and when a
+        // queued survivor needs its subtile, so no register holds it through the unit loop
         const bool c2_live = F.c2_live != 0;
-        const uint64_t tile_base = S.tile_base + local_tile(a.rec[va].v, S.v_first, S.width, S.ntiles);
+        volatile uint64_t &tile_base = item_s[0], &seg_tiles_end = item_s[1];
 
         uint32_t c[3] = {0, 0, 0};
-        uint64_t ctile = UINT64_MAX, t_lo = 1, t_hi = 0;  // this lane's subtile and its v range
+        // this lane's subtile and the end of its v range (a lane's rows rise in v within an item)
+        uint64_t ctile = UINT64_MAX, t_hi = 0;
 
         auto flush = [&]() {                              // populations reduced over lanes of a subtile
             const uint64_t key = (c[0] | c[1] | c[2]) ? ctile : UINT64_MAX - 1 - lane;
@@ -643,14 +650,14 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         };
 
         const uint32_t nrounds = (nv_item + 31) / 32;
-        VRec next;
-        if (warp < nrounds && warp * 32 + lane < nv_item) next = a.rec[va + warp * 32 + lane];
         for (uint32_t r = warp; r < nrounds; r += nwarps) {
             const uint32_t rel = r * 32 + lane;
             const bool active = rel < nv_item;
-            const VRec rec = next;
+            VRec rec{};
+            if (active) rec = a.rec[va + rel];
+            // the record of the next round is prefetched into L1 (no registers held across the round)
             if (r + nwarps < nrounds && rel + nwarps * 32 < nv_item)
-                next = a.rec[va + rel + nwarps * 32];     // prefetch one round ahead
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.rec + va + rel + nwarps * 32));
             // warp-uniform: all 32 rows exist and cover the whole block
             const bool full = r * 32 >= full_lo && r * 32 + 32 <= full_hi;
             int32_t s = 0, e = 0;                         // piece as bits of the block
@@ -659,14 +666,14 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                 e = min((int32_t)(rec.right - block_u0), (int32_t)G::UB);
                 e = max(e, s);
             }
-            const bool moved = active && (rec.v < t_lo || rec.v >= t_hi);
+            const bool moved = active && rec.v >= t_hi;
             if (__any_sync(0xffffffffu, moved)) {
                 flush();
                 if (moved) {
                     const uint64_t stn = S.ntiles, swidth = S.width;
                     const uint64_t lt = local_tile(rec.v, S.v_first, swidth, stn);
                     ctile = lt < stn ? S.tile_base + lt : UINT64_MAX;
-                    t_lo = S.v_first + lt * swidth;
+                    const uint64_t t_lo = S.v_first + lt * swidth;
                     t_hi = lt < stn ? t_lo + swidth : t_lo;
                 }
             }
