@@ -442,7 +442,7 @@ __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bit
 // units that keep a bit after every bitset filter; save receives the bits of the first of them.
 template <int NB, int U, bool FULL, bool C2>
 __device__ __forceinline__ uint32_t piece_units(const uint4 *__restrict__ rows, const uint32_t (&ro)[NB],
-                                                uint32_t lane, int32_t s, int32_t e, uint32_t (&c)[3], uint4 &save) {
+                                                uint32_t lane, int32_t s, int32_t e, uint32_t (&c)[2], uint4 &save) {
     uint32_t pend = 0;
 #pragma unroll
     for (uint32_t p = 0; p < U; ++p) {
@@ -593,22 +593,27 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         const bool c2_live = F.c2_live != 0;
         volatile uint64_t &tile_base = item_s[0], &seg_tiles_end = item_s[1];
 
-        uint32_t c[3] = {0, 0, 0};
-        // this lane's subtile and the end of its v range (a lane's rows rise in v within an item)
-        uint64_t ctile = UINT64_MAX, t_hi = 0;
+        uint32_t c[2] = {0, 0};                           // group 1 and (C2) group 2 survivors of the lane
+        // this lane's subtile as a slot from the item's first one (NO_SLOT: none), and the end of its
+        // v range (a lane's rows rise in v within an item)
+        constexpr uint32_t NO_SLOT = 0xFFFFFFFFu;
+        uint32_t cslot = NO_SLOT;
+        uint64_t t_hi = 0;
 
         auto flush = [&]() {                              // populations reduced over lanes of a subtile
-            const uint64_t key = (c[0] | c[1] | c[2]) ? ctile : UINT64_MAX - 1 - lane;
+            const uint32_t key = (c[0] | c[1]) ? cslot : NO_SLOT - 1 - lane;
             const uint32_t same = __match_any_sync(0xffffffffu, key);
             const uint32_t leader = __ffs(same) - 1;
 #pragma unroll
-            for (int g = 0; g < 3; ++g) {
+            for (int g = 0; g < 2; ++g) {
                 const uint32_t sum = __reduce_add_sync(same, c[g]);
-                if (key == ctile && lane == leader && sum) {
-                    const uint64_t slot = ctile - tile_base;
-                    if (slot < a.tmax) atomicAdd(cnt_s + slot * cstride + 1 + g, sum);
-                    else if (ctile < seg_tiles_end)
-                        atomicAdd((unsigned long long *)&a.counts[ctile * a.stride + 1 + g], (unsigned long long)sum);
+                if (key == cslot && lane == leader && sum) {
+                    if (cslot < a.tmax) atomicAdd(cnt_s + cslot * cstride + 1 + g, sum);
+                    else {
+                        const uint64_t tile = tile_base + cslot;
+                        if (tile < seg_tiles_end)
+                            atomicAdd((unsigned long long *)&a.counts[tile * a.stride + 1 + g], (unsigned long long)sum);
+                    }
                 }
                 c[g] = 0;
             }
@@ -672,7 +677,8 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                 if (moved) {
                     const uint64_t stn = S.ntiles, swidth = S.width;
                     const uint64_t lt = local_tile(rec.v, S.v_first, swidth, stn);
-                    ctile = lt < stn ? S.tile_base + lt : UINT64_MAX;
+                    // slots fit 32 bits (an item's v rows lie in fewer than 2^31 subtiles)
+                    cslot = lt < stn ? (uint32_t)(S.tile_base + lt - tile_base) : NO_SLOT;
                     const uint64_t t_lo = S.v_first + lt * swidth;
                     t_hi = lt < stn ? t_lo + swidth : t_lo;
                 }
@@ -680,8 +686,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             uint32_t ro[NB];                              // unit offset of each filter's row
 #pragma unroll
             for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)(active ? rec.row[f] : 0) * U;
-            const uint64_t slot64 = ctile - tile_base;
-            const uint32_t meta_hi = (slot64 < SLOT_FAR ? (uint32_t)slot64 : SLOT_FAR) << 12;
+            const uint32_t meta_hi = (cslot < SLOT_FAR ? cslot : SLOT_FAR) << 12;
 
             // warp-uniform FULL and block-uniform C2 select the loop body, so the range masks and the
             // group-2 popcounts are not issued (as predicated code) where they cannot apply
