@@ -97,7 +97,7 @@ typedef struct pc_tuning {
     uint32_t block_words;      /* u words (32 u each) staged per CTA: 16, 32 or 64 */
     uint32_t words_per_thread; /* ignored: a lane walks all block_words words of its (v row, block) piece */
     uint32_t v_chunk;          /* v rows per work item (0 = total pieces / (32 x SMs), at least 4 x threads) */
-    uint32_t threads;          /* threads per CTA: 512, 768 or 1024 */
+    uint32_t threads;          /* threads per CTA: 512, 768, 896 or 1024 (0: 896, stepping down to fit) */
     uint32_t deep_records;     /* survivor buffer: deep records per CTA slice (0 = 32768); a run that
                                   needs more reruns once with room for every record */
     uint32_t reserved[2];

@@ -357,7 +357,7 @@ SEARCH_SPACE: dict[str, tuple[int, ...]] = dict(
     width=(1 << 20, 1 << 22, 1 << 24, 1 << 26, 1 << 27),
     bitset_filters=(5, 6, 7, 8),
     block_words=(16, 32, 64),
-    threads=(512, 768, 1024),
+    threads=(512, 768, 896, 1024),
 )
 
 

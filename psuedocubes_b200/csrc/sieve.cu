@@ -404,8 +404,10 @@ __device__ void build_rows(const uint64_t *__restrict__ us, const FamDev &F, uin
 
 constexpr int CBW = 64;                 // bitmap words per cheap-tier filter (q <= 2047)
 constexpr uint64_t ITEM_GRAB = 2;       // fewest work items a CTA claims at a time
-constexpr int QCAP = 64;                // survivor ring per warp (pending < 64 by construction)
-constexpr uint32_t SLOT_FAR = 0xFFFFF;  // queued slot too large to encode: the drain recomputes it
+// Survivor ring per warp (pending < 64 by construction).  An entry is two words: the record's
+// index in the work item (< 2^20) | the bit's position in the block (< 2^12) << 20, and the
+// survivor's subtile slot; v itself is re-read from the record when the ring drains.
+constexpr int QCAP = 64;
 
 __host__ __device__ constexpr uint32_t round16(uint32_t x) { return (x + 15) & ~15u; }
 
@@ -419,7 +421,7 @@ struct MatchSmem {
         rows = 0;
         ures = rows + total_rows * (K / 4) * 16;
         qv = ures + round16(nch * K * 32 * 2);
-        qm = qv + warps * QCAP * 8;
+        qm = qv + warps * QCAP * 4;
         pat = qv;
         const uint32_t ring_end = qm + warps * QCAP * 4, pat_end = pat + nb * PATW * 4;
         cbits = round16(ring_end > pat_end ? ring_end : pat_end);
@@ -498,7 +500,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     char *base = (char *)smem;
     const uint4 *rows = (const uint4 *)(base + L.rows);
     uint16_t *ures = (uint16_t *)(base + L.ures);
-    uint64_t *qv = (uint64_t *)(base + L.qv) + warp * QCAP;
+    uint32_t *qv = (uint32_t *)(base + L.qv) + warp * QCAP;
     uint32_t *qm = (uint32_t *)(base + L.qm) + warp * QCAP;
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
     uint32_t *cbits = (uint32_t *)(base + L.cbits);
@@ -626,18 +628,18 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
         auto drain = [&](uint32_t n) {
             __syncwarp();
             const bool mine = lane < n;
-            uint64_t v = 0;
-            uint32_t meta = 0;
+            uint32_t ent = 0, slot = 0;
             if (mine) {
-                v = qv[(qhead + lane) & (QCAP - 1)];
-                meta = qm[(qhead + lane) & (QCAP - 1)];
+                ent = qv[(qhead + lane) & (QCAP - 1)];
+                slot = qm[(qhead + lane) & (QCAP - 1)];
             }
             __syncwarp();
             qhead += n;
             if (!mine) return;
-            const uint32_t uidx = meta & 0xfff, slot = meta >> 12;
-            const uint64_t tile = slot == SLOT_FAR ? S.tile_base + local_tile(v, S.v_first, S.width, S.ntiles) : tile_base + slot;
+            const uint64_t tile = tile_base + slot;
             if (tile >= seg_tiles_end) return;            // v outside the subtile geometry (reported by k_vprep)
+            const uint32_t uidx = ent >> 20;
+            const uint64_t v = a.rec[va + (ent & 0xFFFFFu)].v;
             for (uint32_t t = 0; t < nch; ++t) {
                 const uint32_t vr = fastmod32(mod64(v, F.cmq[t]) * F.caq[t], F.cmq[t].c, F.cq[t]);
                 int32_t m = (int32_t)ures[t * G::UB + uidx] - (int32_t)vr;
@@ -665,12 +667,9 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(a.rec + va + rel + nwarps * 32));
             // warp-uniform: all 32 rows exist and cover the whole block
             const bool full = r * 32 >= full_lo && r * 32 + 32 <= full_hi;
-            int32_t s = 0, e = 0;                         // piece as bits of the block
-            if (active) {
-                s = max((int32_t)(rec.left - block_u0), 0);
-                e = min((int32_t)(rec.right - block_u0), (int32_t)G::UB);
-                e = max(e, s);
-            }
+            // piece as bits of the block (an inactive lane's zeroed record gives an empty piece)
+            const int32_t s = active ? max((int32_t)(rec.left - block_u0), 0) : 0;
+            const int32_t e = max(min((int32_t)(rec.right - block_u0), (int32_t)G::UB), s);
             const bool moved = active && rec.v >= t_hi;
             if (__any_sync(0xffffffffu, moved)) {
                 flush();
@@ -685,8 +684,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             }
             uint32_t ro[NB];                              // unit offset of each filter's row
 #pragma unroll
-            for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)(active ? rec.row[f] : 0) * U;
-            const uint32_t meta_hi = (cslot < SLOT_FAR ? cslot : SLOT_FAR) << 12;
+            for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)rec.row[f] * U;   // row 0 for an inactive lane
 
             // warp-uniform FULL and block-uniform C2 select the loop body, so the range masks and the
             // group-2 popcounts are not issued (as predicated code) where they cannot apply
@@ -747,8 +745,8 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                             acc.w &= acc.w - 1;
                         }
                         const uint32_t at = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
-                        qv[at] = rec.v;
-                        qm[at] = (u * 128 + bit) | meta_hi;
+                        qv[at] = rel | ((u * 128 + bit) << 20);
+                        qm[at] = cslot;
                     }
                     qtail += __popc(bal);
                     if (qtail - qhead >= 32) drain(32);
@@ -1071,7 +1069,7 @@ uint32_t cheap_count(const pc_filters *f, uint32_t nb) {
 
 // One launch shape for every family of a launch: NB inside every family's bitset range, the cheap
 // tier as deep as the shallowest family allows, shared memory sized by the largest rows and
-// counters.  Defaults: seven bitset filters, 32-word blocks, 1024 threads, stepping down (threads,
+// counters.  Defaults: seven bitset filters, 32-word blocks, 896 threads, stepping down (threads,
 // then block words, then bitset filters) until the layout fits the opt-in shared memory.
 int resolve_tuning(pc_ctx *ctx, const std::vector<const pc_filters *> &fams, const pc_tuning *t, Tuned &r,
                    size_t &smem, uint32_t &tmax) {
@@ -1088,8 +1086,8 @@ int resolve_tuning(pc_ctx *ctx, const std::vector<const pc_filters *> &fams, con
     r.K = t && t->block_words ? t->block_words : 32;
     if (r.K != 16 && r.K != 32 && r.K != 64) r.K = 32;
     const bool fixed_threads = t && t->threads;
-    r.threads = fixed_threads ? t->threads : 1024;
-    if (r.threads != 512 && r.threads != 768 && r.threads != 1024) r.threads = 512;
+    r.threads = fixed_threads ? t->threads : 896;
+    if (r.threads != 512 && r.threads != 768 && r.threads != 896 && r.threads != 1024) r.threads = 512;
     r.v_chunk = t ? t->v_chunk : 0;
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
@@ -1109,7 +1107,7 @@ int resolve_tuning(pc_ctx *ctx, const std::vector<const pc_filters *> &fams, con
                 return PC_OK;
             }
         }
-        if (!fixed_threads && r.threads > 512) r.threads = r.threads == 1024 ? 768 : 512;
+        if (!fixed_threads && r.threads > 512) r.threads = r.threads > 896 ? 896 : r.threads == 896 ? 768 : 512;
         else if (r.K > 16) r.K /= 2;
         else if (r.nb > nb_lo) r.nb--;
         else return pc_fail(ctx, PC_INVALID, "residual rows do not fit shared memory");
@@ -1256,6 +1254,7 @@ int engine_match(Engine &E, int mode) {
     ma.deep_count = E.d_deep_count;
     ma.item_next = E.d_item_next;
     if (E.tn.threads == 1024) return launch_match_n<1024>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
+    if (E.tn.threads == 896) return launch_match_n<896>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
     if (E.tn.threads == 768) return launch_match_n<768>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
     return launch_match_n<512>(E.ctx, ma, E.tn.nb, E.tn.K, E.smem, E.grid, mode);
 }

@@ -139,6 +139,10 @@ def test_every_tuning_gives_identical_batches(runtime, p619, focuses619):
                 got = MaskedMatcher(runtime, p619, dict(bitset_filters=nb, block_words=K, v_chunk=chunk)).run(batch)
                 compare(base, got)
                 assert got['subtile_scopes'] == base['subtile_scopes']
+    for threads in (512, 768, 896, 1024):
+        got = MaskedMatcher(runtime, p619, dict(bitset_filters=7, block_words=32, threads=threads)).run(batch)
+        compare(base, got)
+        assert got['subtile_scopes'] == base['subtile_scopes']
 
 
 def test_golden_lease(runtime, p619, focuses619):
