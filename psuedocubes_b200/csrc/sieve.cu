@@ -674,12 +674,21 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             if (__any_sync(0xffffffffu, moved)) {
                 flush();
                 if (moved) {
-                    const uint64_t stn = S.ntiles, swidth = S.width;
-                    const uint64_t lt = local_tile(rec.v, S.v_first, swidth, stn);
-                    // slots fit 32 bits (an item's v rows lie in fewer than 2^31 subtiles)
-                    cslot = lt < stn ? (uint32_t)(S.tile_base + lt - tile_base) : NO_SLOT;
-                    const uint64_t t_lo = S.v_first + lt * swidth;
-                    t_hi = lt < stn ? t_lo + swidth : t_lo;
+                    const uint64_t swidth = S.width;
+                    if (cslot != NO_SLOT && rec.v - t_hi < 2 * swidth) {
+                        // the next subtile or the one after it (the common step between rounds)
+                        const bool two = rec.v - t_hi >= swidth;
+                        cslot += two ? 2 : 1;
+                        t_hi += two ? 2 * swidth : swidth;
+                        if ((uint64_t)(tile_base + cslot) >= seg_tiles_end) cslot = NO_SLOT, t_hi = 0;
+                    } else {
+                        const uint64_t stn = S.ntiles;
+                        const uint64_t lt = local_tile(rec.v, S.v_first, swidth, stn);
+                        // slots fit 32 bits (an item's v rows lie in fewer than 2^31 subtiles)
+                        cslot = lt < stn ? (uint32_t)(S.tile_base + lt - tile_base) : NO_SLOT;
+                        const uint64_t t_lo = S.v_first + lt * swidth;
+                        t_hi = lt < stn ? t_lo + swidth : t_lo;
+                    }
                 }
             }
             uint32_t ro[NB];                              // unit offset of each filter's row
