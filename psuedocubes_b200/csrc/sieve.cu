@@ -89,6 +89,7 @@ struct FamDev {
 struct MatchArgs {
     const uint64_t *us;
     const VRec *rec;
+    const uint64_t *cres;            // per v: cheap-tier residues v*A mod q, 16 bits each
     const SegDev *seg;
     const FamDev *fam;
     const uint32_t *blk_seg;         // per u block: its segment
@@ -185,6 +186,8 @@ struct PrepArgs {
     const FamDev *fam;
     uint32_t nb, stride;
     VRec *rec;
+    uint64_t *cres;                  // per v: v*A mod q of the cheap-tier filters, 16 bits each
+    uint32_t nch;
     uint64_t *counts;
     unsigned long long *bad;
 };
@@ -263,6 +266,11 @@ __global__ void k_vprep(const PrepArgs a) {
         for (int f = 0; f < PC_MAX_BITSET; ++f)
             r.row[f] = f < (int)a.nb ? (uint16_t)(F.row0[f] + mod64(v, F.mq[f])) : (uint16_t)0;
         a.rec[j] = r;
+        uint64_t cr = 0;
+#pragma unroll
+        for (int t = 0; t < PC_MAX_CHEAP; ++t)
+            if (t < (int)a.nch) cr |= (uint64_t)fastmod32(mod64(v, F.cmq[t]) * F.caq[t], F.cmq[t].c, F.cq[t]) << (16 * t);
+        a.cres[j] = cr;
         pop += right - left;
     }
     if (tile != UINT64_MAX && pop) atomicAdd((unsigned long long *)&a.counts[tile * a.stride], (unsigned long long)pop);
@@ -408,6 +416,10 @@ constexpr uint64_t ITEM_GRAB = 2;       // fewest work items a CTA claims at a t
 // index in the work item (< 2^20) | the bit's position in the block (< 2^12) << 20, and the
 // survivor's subtile slot; v itself is re-read from the record when the ring drains.
 constexpr int QCAP = 64;
+// Leftover list per warp: a piece's marked units after its first, as the record's index in the
+// work item | the unit << 20 | the subtile slot << 24 (255: recomputed from v), recomputed 32 at a
+// time so the round loop does not wait on a few lanes.
+constexpr int LCAP = 32;
 
 __host__ __device__ constexpr uint32_t round16(uint32_t x) { return (x + 15) & ~15u; }
 
@@ -415,15 +427,16 @@ __host__ __device__ constexpr uint32_t round16(uint32_t x) { return (x + 15) & ~
 // residue-row patterns are only read while rows are built, when every survivor ring is empty,
 // so they share the rings' space.
 struct MatchSmem {
-    uint32_t rows, ures, qv, qm, pat, cbits, cnt, fam, seg, misc, total;
+    uint32_t rows, ures, qv, qm, lq, pat, cbits, cnt, fam, seg, misc, total;
     __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t nch, uint32_t tmax,
                                   uint32_t ng, uint32_t warps) {
         rows = 0;
         ures = rows + total_rows * (K / 4) * 16;
         qv = ures + round16(nch * K * 32 * 2);
         qm = qv + warps * QCAP * 4;
+        lq = qm + warps * QCAP * 4;
         pat = qv;
-        const uint32_t ring_end = qm + warps * QCAP * 4, pat_end = pat + nb * PATW * 4;
+        const uint32_t ring_end = lq + warps * LCAP * 4, pat_end = pat + nb * PATW * 4;
         cbits = round16(ring_end > pat_end ? ring_end : pat_end);
         cnt = cbits + nch * CBW * 4;
         fam = cnt + round16(tmax * (ng + 2) * 4);
@@ -502,6 +515,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     uint16_t *ures = (uint16_t *)(base + L.ures);
     uint32_t *qv = (uint32_t *)(base + L.qv) + warp * QCAP;
     uint32_t *qm = (uint32_t *)(base + L.qm) + warp * QCAP;
+    uint32_t *lq = (uint32_t *)(base + L.lq) + warp * LCAP;
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
     uint32_t *cbits = (uint32_t *)(base + L.cbits);
     uint32_t *cnt_s = (uint32_t *)(base + L.cnt);      // tmax x (ngmax+2): groups 1..ng
@@ -639,9 +653,9 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const uint64_t tile = tile_base + slot;
             if (tile >= seg_tiles_end) return;            // v outside the subtile geometry (reported by k_vprep)
             const uint32_t uidx = ent >> 20;
-            const uint64_t v = a.rec[va + (ent & 0xFFFFFu)].v;
+            const uint64_t cr = a.cres[va + (ent & 0xFFFFFu)];
             for (uint32_t t = 0; t < nch; ++t) {
-                const uint32_t vr = fastmod32(mod64(v, F.cmq[t]) * F.caq[t], F.cmq[t].c, F.cq[t]);
+                const uint32_t vr = (uint32_t)(cr >> (16 * t)) & 0xFFFFu;
                 int32_t m = (int32_t)ures[t * G::UB + uidx] - (int32_t)vr;
                 if (m < 0) m += (int32_t)F.cq[t];
                 if (!((cbits[t * CBW + (m >> 5)] >> (m & 31)) & 1u)) return;
@@ -652,19 +666,86 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                 }
             }
             const uint32_t at = atomicAdd(deep_ctr, 1u);
-            if (at < a.deep_cap)
+            if (at < a.deep_cap) {
+                const uint64_t v = a.rec[va + (ent & 0xFFFFFu)].v;
                 deep_slice[at] = make_uint4((uint32_t)v, (uint32_t)(v >> 32), block_u0 + uidx, (uint32_t)tile);
+            }
         };
 
-        const uint32_t nrounds = (nv_item + 31) / 32;
-        for (uint32_t r = warp; r < nrounds; r += nwarps) {
+        // The bits of one unit per lane go to the ring, one bit per lane per step (warp-uniform call).
+        auto queue_bits = [&](uint4 acc, uint32_t u, uint32_t rel, uint32_t slot) {
+            while (__any_sync(0xffffffffu, (acc.x | acc.y | acc.z | acc.w) != 0)) {
+                const bool has = (acc.x | acc.y | acc.z | acc.w) != 0;
+                const uint32_t bal = __ballot_sync(0xffffffffu, has);
+                if (has) {
+                    uint32_t bit;
+                    if (acc.x) {
+                        bit = __ffs(acc.x) - 1;
+                        acc.x &= acc.x - 1;
+                    } else if (acc.y) {
+                        bit = 32 + __ffs(acc.y) - 1;
+                        acc.y &= acc.y - 1;
+                    } else if (acc.z) {
+                        bit = 64 + __ffs(acc.z) - 1;
+                        acc.z &= acc.z - 1;
+                    } else {
+                        bit = 96 + __ffs(acc.w) - 1;
+                        acc.w &= acc.w - 1;
+                    }
+                    const uint32_t at = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
+                    qv[at] = rel | ((u * 128 + bit) << 20);
+                    qm[at] = slot;
+                }
+                qtail += __popc(bal);
+                if (qtail - qhead >= 32) drain(32);
+            }
+        };
+
+        uint32_t nl = 0;                                  // warp-uniform leftover count
+        // Up to 32 leftover units, one per lane: recomputed from the record, bits queued.
+        auto leftovers = [&]() {
+            __syncwarp();
+            const bool mine = lane < nl;
+            const uint32_t ent = mine ? lq[lane] : 0u;
+            __syncwarp();
+            nl = 0;
+            uint4 acc = make_uint4(0, 0, 0, 0);
+            const uint32_t rel = ent & 0xFFFFFu, u = (ent >> 20) & 0xFu;
+            uint32_t slot = ent >> 24;
+            if (mine) {
+                const VRec rr = a.rec[va + rel];
+                if (slot == 255u) {
+                    const uint64_t lt = local_tile(rr.v, S.v_first, S.width, S.ntiles);
+                    slot = lt < S.ntiles ? (uint32_t)(S.tile_base + lt - tile_base) : NO_SLOT;
+                }
+                acc = rows[(uint32_t)rr.row[0] * U + u];
+#pragma unroll
+                for (int f = 1; f < NB; ++f) {
+                    const uint4 w = rows[(uint32_t)rr.row[f] * U + u];
+                    acc.x &= w.x;
+                    acc.y &= w.y;
+                    acc.z &= w.z;
+                    acc.w &= w.w;
+                }
+                const int32_t s = max((int32_t)(rr.left - block_u0), 0);
+                const int32_t e = max(min((int32_t)(rr.right - block_u0), (int32_t)G::UB), s);
+                const int32_t lo = s - (int32_t)u * 128, hi = e - (int32_t)u * 128;
+                acc.x &= unit_mask(lo, hi), acc.y &= unit_mask(lo - 32, hi - 32);
+                acc.z &= unit_mask(lo - 64, hi - 64), acc.w &= unit_mask(lo - 96, hi - 96);
+            }
+            queue_bits(acc, u, rel, slot);
+        };
+
+        // a warp takes consecutive rounds, so its lanes stay in one subtile for many rounds
+        const uint32_t nrounds = (nv_item + 31) / 32, per_warp = (nrounds + nwarps - 1) / nwarps;
+        const uint32_t r_end = min(nrounds, (warp + 1) * per_warp);
+        for (uint32_t r = warp * per_warp; r < r_end; ++r) {
             const uint32_t rel = r * 32 + lane;
             const bool active = rel < nv_item;
             VRec rec{};
             if (active) rec = a.rec[va + rel];
             // the record of the next round is prefetched into L1 (no registers held across the round)
-            if (r + nwarps < nrounds && rel + nwarps * 32 < nv_item)
-                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.rec + va + rel + nwarps * 32));
+            if (r + 1 < r_end && rel + 32 < nv_item) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.rec + va + rel + 32));
             // warp-uniform: all 32 rows exist and cover the whole block
             const bool full = r * 32 >= full_lo && r * 32 + 32 <= full_hi;
             // piece as bits of the block (an inactive lane's zeroed record gives an empty piece)
@@ -705,63 +786,29 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             else
                 pend = c2_live ? piece_units<NB, U, false, true>(rows, ro, lane, s, e, c, save)
                                : piece_units<NB, U, false, false>(rows, ro, lane, s, e, c, save);
-            bool saved = pend != 0;                       // the next marked unit is the saved one
-            while (__any_sync(0xffffffffu, pend != 0)) {      // recompute a marked unit, queue its bits
-                uint4 acc = make_uint4(0, 0, 0, 0);
-                uint32_t u = 0;
-                const bool again = pend != 0 && !saved;
-                if (saved) {
-                    const uint32_t p = __ffs(pend) - 1;
+            // the first marked unit (its bits kept in registers) is queued now; the piece's further
+            // marked units go to the leftover list
+            uint4 acc = make_uint4(0, 0, 0, 0);
+            uint32_t u = 0;
+            if (pend) {
+                u = (lane + __ffs(pend) - 1) & (U - 1);
+                acc = save;
+                pend &= pend - 1;
+            }
+            queue_bits(acc, u, rel, cslot);
+            while (__any_sync(0xffffffffu, pend != 0)) {
+                const bool has = pend != 0;
+                const uint32_t bal = __ballot_sync(0xffffffffu, has);
+                if (nl + __popc(bal) > LCAP) leftovers();
+                if (has) {
+                    lq[nl + __popc(bal & lanes_below)] =
+                        rel | (((lane + __ffs(pend) - 1) & (U - 1)) << 20) | (min(cslot, 255u) << 24);
                     pend &= pend - 1;
-                    u = (lane + p) & (U - 1);
-                    acc = save;
-                    saved = false;
-                } else if (again) {
-                    const uint32_t p = __ffs(pend) - 1;
-                    pend &= pend - 1;
-                    u = (lane + p) & (U - 1);
-                    acc = rows[ro[0] + u];
-#pragma unroll
-                    for (int f = 1; f < NB; ++f) {
-                        const uint4 w = rows[ro[f] + u];
-                        acc.x &= w.x;
-                        acc.y &= w.y;
-                        acc.z &= w.z;
-                        acc.w &= w.w;
-                    }
-                    if (!full) {
-                        const int32_t lo = s - (int32_t)u * 128, hi = e - (int32_t)u * 128;
-                        acc.x &= unit_mask(lo, hi), acc.y &= unit_mask(lo - 32, hi - 32);
-                        acc.z &= unit_mask(lo - 64, hi - 64), acc.w &= unit_mask(lo - 96, hi - 96);
-                    }
                 }
-                while (__any_sync(0xffffffffu, (acc.x | acc.y | acc.z | acc.w) != 0)) {
-                    const bool has = (acc.x | acc.y | acc.z | acc.w) != 0;
-                    const uint32_t bal = __ballot_sync(0xffffffffu, has);
-                    if (has) {
-                        uint32_t bit;
-                        if (acc.x) {
-                            bit = __ffs(acc.x) - 1;
-                            acc.x &= acc.x - 1;
-                        } else if (acc.y) {
-                            bit = 32 + __ffs(acc.y) - 1;
-                            acc.y &= acc.y - 1;
-                        } else if (acc.z) {
-                            bit = 64 + __ffs(acc.z) - 1;
-                            acc.z &= acc.z - 1;
-                        } else {
-                            bit = 96 + __ffs(acc.w) - 1;
-                            acc.w &= acc.w - 1;
-                        }
-                        const uint32_t at = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
-                        qv[at] = rel | ((u * 128 + bit) << 20);
-                        qm[at] = cslot;
-                    }
-                    qtail += __popc(bal);
-                    if (qtail - qhead >= 32) drain(32);
-                }
+                nl += __popc(bal);
             }
         }
+        if (nl) leftovers();
         if (qtail != qhead) drain(qtail - qhead);
         flush();
         __syncthreads();
@@ -1176,6 +1223,7 @@ struct Engine {
     uint64_t *d_counts = nullptr, *d_geo = nullptr, *d_out = nullptr;
     unsigned long long *d_nout = nullptr;                 // [0] outputs, [1] rows outside the geometry
     VRec *d_rec = nullptr;
+    uint64_t *d_cres = nullptr;
     uint4 *d_bv = nullptr;
     uint64_t *d_pieces = nullptr, *d_tmp = nullptr, *d_items = nullptr, *d_prefix = nullptr, *d_vchunk = nullptr;
     uint64_t *d_ws = nullptr;
@@ -1220,6 +1268,7 @@ int engine_prepare(Engine &E, const pc_tuning *tuning, Scratch &hold) {
     if (!rc) rc = hold.get(&E.d_out, 2 * std::max<uint64_t>(1, E.out_cap));
     if (!rc) rc = hold.get(&E.d_nout, 2);
     if (!rc) rc = hold.get(&E.d_rec, std::max<uint64_t>(1, E.nv));
+    if (!rc) rc = hold.get(&E.d_cres, std::max<uint64_t>(1, E.nv));
     if (!rc) rc = hold.get(&E.d_bv, nb1);
     if (!rc) rc = hold.get(&E.d_blk_seg, nb1);
     if (!rc) rc = hold.get(&E.d_pieces, nb1);
@@ -1245,6 +1294,7 @@ int engine_match(Engine &E, int mode) {
     MatchArgs ma{};
     ma.us = E.us;
     ma.rec = E.d_rec;
+    ma.cres = E.d_cres;
     ma.seg = E.d_seg;
     ma.fam = E.d_fam;
     ma.blk_seg = E.d_blk_seg;
@@ -1288,6 +1338,8 @@ int engine_front(Engine &E, bool events, bool capturing, int *launches) {
         pa.nb = E.tn.nb;
         pa.stride = E.stride;
         pa.rec = E.d_rec;
+        pa.cres = E.d_cres;
+        pa.nch = E.tn.nch;
         pa.counts = E.d_counts;
         pa.bad = E.d_nout + 1;
         const uint64_t runs = (E.nv + PREP_RUN - 1) / PREP_RUN;
