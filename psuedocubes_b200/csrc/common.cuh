@@ -196,6 +196,32 @@ __device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane) {
     return x;
 }
 
+// The same transpose with its per-lane constants computed once: in exchange round r (block size
+// j = 16 >> r) a lane rotates its partner's word by sh[r] (left by j for the lower lane of a pair,
+// right by j for the upper one) and keeps its own bits where keep[r] is set, one funnel shift and
+// one bit-select per round.
+__device__ __forceinline__ void transpose_consts(uint32_t lane, uint32_t (&sh)[5], uint32_t (&keep)[5]) {
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        const uint32_t j = 16u >> r;
+        const uint32_t hm = r == 0 ? 0xffff0000u : r == 1 ? 0xff00ff00u : r == 2 ? 0xf0f0f0f0u
+                          : r == 3 ? 0xccccccccu : 0xaaaaaaaau;
+        const bool upper = lane & j;
+        sh[r] = upper ? 32u - j : j;
+        keep[r] = upper ? hm : ~hm;
+    }
+}
+
+__device__ __forceinline__ uint32_t transpose32c(uint32_t x, const uint32_t (&sh)[5], const uint32_t (&keep)[5]) {
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        const uint32_t p = __shfl_xor_sync(0xffffffffu, x, 16u >> r);
+        const uint32_t moved = __funnelshift_l(p, p, sh[r]);
+        x = (x & keep[r]) | (moved & ~keep[r]);
+    }
+    return x;
+}
+
 // ------------------------------------------------------------------------------------------
 // internal host helpers shared across translation units
 

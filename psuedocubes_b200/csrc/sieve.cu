@@ -381,15 +381,21 @@ __device__ void build_rows(const uint64_t *__restrict__ us, const FamDev &F, uin
         for (uint32_t t = 0; t < nch; ++t)
             ures[t * G::UB + k] = (uint16_t)fastmod32(mod64(u, F.cmq[t]) * F.cbq[t], F.cmq[t].c, F.cq[t]);
     }
-    // a warp builds all q rows of one filter for one 16-byte unit (4 words = 128 u)
-    for (uint32_t pair = warp; pair < NB * G::U; pair += nwarps) {
-        const uint32_t f = pair / G::U, c = pair % G::U;
+    // A warp builds all q rows of one filter for two 16-byte units, c and c + U/2 (4 words = 128 u
+    // each).  Its lanes store the two units in two steps, half the lanes writing each unit, so a
+    // quarter-warp store meets two bank groups instead of one.
+    uint32_t sh[5], keep[5];                              // per-lane transpose constants
+    transpose_consts(lane, sh, keep);
+    constexpr uint32_t HU = G::U / 2;
+    const bool hi_first = lane & 4;
+    for (uint32_t item = warp; item < NB * HU; item += nwarps) {
+        const uint32_t f = item / HU, c = item % HU;
         const uint32_t q = F.q[f];
-        uint32_t t[4];
-        bool valid[4];
+        uint32_t t[8];
+        bool valid[8];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint32_t local = (c * 4 + k) * 32 + lane;
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t local = ((c + (k >> 2) * HU) * 4 + (k & 3)) * 32 + lane;
             valid[k] = local < n_valid;
             const uint32_t um = valid[k] ? mod64(__ldg(ub + local), F.mq[f]) : 0;
             t[k] = fastmod32(um * F.ainvb[f], F.mq[f].c, q);
@@ -397,15 +403,19 @@ __device__ void build_rows(const uint64_t *__restrict__ us, const FamDev &F, uin
         const uint32_t *p = pat_s + f * PATW;
         const uint32_t row0 = F.row0[f];
         for (uint32_t g = 0; g * 32 < q; ++g) {
-            uint32_t w[4];
+            uint32_t w[8];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < 8; ++k) {
                 const uint32_t st = 32 * g + q - t[k];
                 const uint32_t col = __funnelshift_r(p[st >> 5], p[(st >> 5) + 1], st & 31);
-                w[k] = transpose32(valid[k] ? col : 0u, lane);
+                w[k] = transpose32c(valid[k] ? col : 0u, sh, keep);
             }
             const uint32_t r = 32 * g + lane;
-            if (r < q) rows[G::unit(row0 + r, c)] = make_uint4(w[0], w[1], w[2], w[3]);
+            if (r < q) {
+                const uint4 lo = make_uint4(w[0], w[1], w[2], w[3]), hi = make_uint4(w[4], w[5], w[6], w[7]);
+                rows[G::unit(row0 + r, hi_first ? c + HU : c)] = hi_first ? hi : lo;
+                rows[G::unit(row0 + r, hi_first ? c : c + HU)] = hi_first ? lo : hi;
+            }
         }
     }
 }
