@@ -465,19 +465,25 @@ __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bit
 // unless the row covers the whole block (FULL), the group-1 popcount (first four filters) and,
 // when group 2 ends at the last bitset filter (C2), the group-2 popcount.  Returns the mask of
 // units that keep a bit after every bitset filter; save receives the bits of the first of them.
+__device__ __forceinline__ uint4 lds128(uint32_t addr) {      // 16-byte shared-memory load
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
+    return v;
+}
+
 template <int NB, int U, bool FULL, bool C2>
-__device__ __forceinline__ uint32_t piece_units(const uint4 *__restrict__ rows, const uint32_t (&ro)[NB],
-                                                uint32_t lane, int32_t s, int32_t e, uint32_t (&c)[2], uint4 &save) {
+__device__ __forceinline__ uint32_t piece_units(const uint32_t (&rb)[NB], uint32_t lane, int32_t s, int32_t e,
+                                                uint32_t (&c)[2], uint4 &save) {
     uint32_t pend = 0;
 #pragma unroll
     for (uint32_t p = 0; p < U; ++p) {
-        const uint32_t u = (lane + p) & (U - 1);
-        uint4 acc = rows[ro[0] + u];
+        const uint32_t u = (lane + p) & (U - 1), uo = u * 16;
+        uint4 acc = lds128(rb[0] + uo);
         uint4 acc4;
 #pragma unroll
         for (int f = 1; f < NB; ++f) {
             if (f == 4) acc4 = acc;
-            const uint4 w = rows[ro[f] + u];
+            const uint4 w = lds128(rb[f] + uo);
             acc.x &= w.x;
             acc.y &= w.y;
             acc.z &= w.z;
@@ -494,7 +500,7 @@ __device__ __forceinline__ uint32_t piece_units(const uint4 *__restrict__ rows, 
         c[0] += __popc(acc4.x) + __popc(acc4.y) + __popc(acc4.z) + __popc(acc4.w);
         if (C2) c[1] += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
         const bool live = (acc.x | acc.y | acc.z | acc.w) != 0;
-        if (live && !pend) save = acc;                // the first marked unit is not read again
+        if (live) save = acc;                         // the last marked unit is not read again
         pend |= (uint32_t)live << p;
     }
     return pend;
@@ -522,6 +528,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     const MatchSmem L(a.total_rows, K, NB, a.nch, a.tmax, ngmax, nwarps);
     char *base = (char *)smem;
     const uint4 *rows = (const uint4 *)(base + L.rows);
+    const uint32_t rows_addr = (uint32_t)__cvta_generic_to_shared(rows);
     uint16_t *ures = (uint16_t *)(base + L.ures);
     uint32_t *qv = (uint32_t *)(base + L.qv) + warp * QCAP;
     uint32_t *qm = (uint32_t *)(base + L.qm) + warp * QCAP;
@@ -782,28 +789,29 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                     }
                 }
             }
-            uint32_t ro[NB];                              // unit offset of each filter's row
+            uint32_t rb[NB];                              // shared address of each filter's row
 #pragma unroll
-            for (int f = 0; f < NB; ++f) ro[f] = (uint32_t)rec.row[f] * U;   // row 0 for an inactive lane
+            for (int f = 0; f < NB; ++f) rb[f] = rows_addr + (uint32_t)rec.row[f] * (U * 16);   // row 0 if inactive
 
             // warp-uniform FULL and block-uniform C2 select the loop body, so the range masks and the
             // group-2 popcounts are not issued (as predicated code) where they cannot apply
             uint32_t pend;                                // units of this piece with survivors
             uint4 save;                                   // bits of its first one
             if (full)
-                pend = c2_live ? piece_units<NB, U, true, true>(rows, ro, lane, s, e, c, save)
-                               : piece_units<NB, U, true, false>(rows, ro, lane, s, e, c, save);
+                pend = c2_live ? piece_units<NB, U, true, true>(rb, lane, s, e, c, save)
+                               : piece_units<NB, U, true, false>(rb, lane, s, e, c, save);
             else
-                pend = c2_live ? piece_units<NB, U, false, true>(rows, ro, lane, s, e, c, save)
-                               : piece_units<NB, U, false, false>(rows, ro, lane, s, e, c, save);
-            // the first marked unit (its bits kept in registers) is queued now; the piece's further
+                pend = c2_live ? piece_units<NB, U, false, true>(rb, lane, s, e, c, save)
+                               : piece_units<NB, U, false, false>(rb, lane, s, e, c, save);
+            // the last marked unit (its bits kept in registers) is queued now; the piece's other
             // marked units go to the leftover list
             uint4 acc = make_uint4(0, 0, 0, 0);
             uint32_t u = 0;
             if (pend) {
-                u = (lane + __ffs(pend) - 1) & (U - 1);
+                const uint32_t pl = 31 - __clz(pend);
+                u = (lane + pl) & (U - 1);
                 acc = save;
-                pend &= pend - 1;
+                pend &= ~(1u << pl);
             }
             queue_bits(acc, u, rel, cslot);
             while (__any_sync(0xffffffffu, pend != 0)) {
