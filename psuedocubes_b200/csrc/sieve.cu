@@ -422,9 +422,9 @@ __device__ void build_rows(const uint64_t *__restrict__ us, const FamDev &F, uin
 
 constexpr int CBW = 64;                 // bitmap words per cheap-tier filter (q <= 2047)
 constexpr uint64_t ITEM_GRAB = 2;       // fewest work items a CTA claims at a time
-// Survivor ring per warp (pending < 64 by construction).  An entry is two words: the record's
+// Survivor ring per warp (pending < 64 by construction).  An entry is one word pair: the record's
 // index in the work item (< 2^20) | the bit's position in the block (< 2^12) << 20, and the
-// survivor's subtile slot; v itself is re-read from the record when the ring drains.
+// survivor's subtile slot; the drain reads the v row's cheap-tier residues by the record index.
 constexpr int QCAP = 64;
 // Leftover list per warp: a piece's marked units after its first, as the record's index in the
 // work item | the unit << 20 | the subtile slot << 24 (255: recomputed from v), recomputed 32 at a
@@ -437,15 +437,14 @@ __host__ __device__ constexpr uint32_t round16(uint32_t x) { return (x + 15) & ~
 // residue-row patterns are only read while rows are built, when every survivor ring is empty,
 // so they share the rings' space.
 struct MatchSmem {
-    uint32_t rows, ures, qv, qm, lq, pat, cbits, cnt, fam, seg, misc, total;
+    uint32_t rows, ures, ring, lq, pat, cbits, cnt, fam, seg, misc, total;
     __host__ __device__ MatchSmem(uint32_t total_rows, uint32_t K, uint32_t nb, uint32_t nch, uint32_t tmax,
                                   uint32_t ng, uint32_t warps) {
         rows = 0;
         ures = rows + total_rows * (K / 4) * 16;
-        qv = ures + round16(nch * K * 32 * 2);
-        qm = qv + warps * QCAP * 4;
-        lq = qm + warps * QCAP * 4;
-        pat = qv;
+        ring = ures + round16(nch * K * 32 * 2);
+        lq = ring + warps * QCAP * 8;
+        pat = ring;
         const uint32_t ring_end = lq + warps * LCAP * 4, pat_end = pat + nb * PATW * 4;
         cbits = round16(ring_end > pat_end ? ring_end : pat_end);
         cnt = cbits + nch * CBW * 4;
@@ -530,8 +529,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     const uint4 *rows = (const uint4 *)(base + L.rows);
     const uint32_t rows_addr = (uint32_t)__cvta_generic_to_shared(rows);
     uint16_t *ures = (uint16_t *)(base + L.ures);
-    uint32_t *qv = (uint32_t *)(base + L.qv) + warp * QCAP;
-    uint32_t *qm = (uint32_t *)(base + L.qm) + warp * QCAP;
+    uint2 *qv = (uint2 *)(base + L.ring) + warp * QCAP;
     uint32_t *lq = (uint32_t *)(base + L.lq) + warp * LCAP;
     uint32_t *pat_s = (uint32_t *)(base + L.pat);
     uint32_t *cbits = (uint32_t *)(base + L.cbits);
@@ -661,8 +659,8 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const bool mine = lane < n;
             uint32_t ent = 0, slot = 0;
             if (mine) {
-                ent = qv[(qhead + lane) & (QCAP - 1)];
-                slot = qm[(qhead + lane) & (QCAP - 1)];
+                const uint2 q = qv[(qhead + lane) & (QCAP - 1)];
+                ent = q.x, slot = q.y;
             }
             __syncwarp();
             qhead += n;
@@ -710,8 +708,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                         acc.w &= acc.w - 1;
                     }
                     const uint32_t at = (qtail + __popc(bal & lanes_below)) & (QCAP - 1);
-                    qv[at] = rel | ((u * 128 + bit) << 20);
-                    qm[at] = slot;
+                    qv[at] = make_uint2(rel | ((u * 128 + bit) << 20), slot);
                 }
                 qtail += __popc(bal);
                 if (qtail - qhead >= 32) drain(32);
