@@ -352,7 +352,7 @@ class WindowBatch:
 
 #: the autotuner's choice for the 512 seeded uneven windows (p in [499, 619]) on a B200; a batch
 #: whose deep survivors outgrow deep_records per CTA is rerun larger when it runs eagerly
-DEFAULT_SETTINGS: dict[str, int] = dict(width=1 << 27, bitset_filters=7, block_words=32, threads=768, deep_records=8192)
+DEFAULT_SETTINGS: dict[str, int] = dict(width=1 << 27, bitset_filters=7, block_words=32, threads=896, deep_records=8192)
 SEARCH_SPACE: dict[str, tuple[int, ...]] = dict(
     width=(1 << 20, 1 << 22, 1 << 24, 1 << 26, 1 << 27),
     bitset_filters=(5, 6, 7, 8),
