@@ -193,7 +193,8 @@ struct PrepArgs {
 };
 
 // Per v row: exact u interval as list indices (batch_experiment.py:209-215), bitset row
-// indices, and the focused-position count of its subtile.  A thread owns PREP_RUN consecutive v
+// indices, the residues v*A mod q of the cheap-tier filters, and the focused-position count of
+// its subtile.  A thread owns PREP_RUN consecutive v
 // rows: one binary search per bound for the first row of each segment, then the monotone bounds
 // advance linearly (about N_u/N_v < 1 step per row).
 constexpr int PREP_RUN = 16;
@@ -460,16 +461,17 @@ __device__ __forceinline__ uint32_t unit_mask(int32_t lo, int32_t hi) {   // bit
     return low_bits((uint32_t)min(max(hi, 0), 32)) & ~low_bits((uint32_t)min(max(lo, 0), 32));
 }
 
-// The unit loop of one (v row, block) piece: AND of the NB rows per 16-byte unit, range masks
-// unless the row covers the whole block (FULL), the group-1 popcount (first four filters) and,
-// when group 2 ends at the last bitset filter (C2), the group-2 popcount.  Returns the mask of
-// units that keep a bit after every bitset filter; save receives the bits of the first of them.
 __device__ __forceinline__ uint4 lds128(uint32_t addr) {      // 16-byte shared-memory load
     uint4 v;
     asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
     return v;
 }
 
+// The unit loop of one (v row, block) piece, from the shared address of each filter's row: AND of
+// the NB rows per 16-byte unit, range masks unless the row covers the whole block (FULL), the
+// group-1 popcount (first four filters) and, when group 2 ends at the last bitset filter (C2), the
+// group-2 popcount.  Returns the mask of units that keep a bit after every bitset filter; save
+// receives the bits of the last of them.
 template <int NB, int U, bool FULL, bool C2>
 __device__ __forceinline__ uint32_t piece_units(const uint32_t (&rb)[NB], uint32_t lane, int32_t s, int32_t e,
                                                 uint32_t (&c)[2], uint4 &save) {
@@ -511,12 +513,12 @@ __device__ __forceinline__ void copy_words(void *dst, const void *src, uint32_t 
 
 // One lane owns one (v row, u block) piece: it walks the block's K/4 16-byte units in the order
 // (lane + p) mod (K/4), so at every step the 32 lanes of a warp hit each 16-byte bank group
-// exactly 32/(K/4) times whatever rows they read.  Group counters of groups 1..3 live in
-// registers (c[0..2]) and are reduced per subtile when a lane's subtile changes.  The unit loop
-// only marks the units that keep a bit after every bitset filter (and keeps the bits of the
-// first one in registers); once the piece is done, the lanes take their marked units (the first
-// from registers, any further one re-read) and queue the bits, so the warp votes and diverges
-// once per piece instead of after every unit.
+// exactly 32/(K/4) times whatever rows they read.  The group-1 and group-2 counters live in
+// registers (c[0..1]) and are reduced per subtile when a lane's subtile changes.  The unit loop
+// only marks the units that keep a bit after every bitset filter (and keeps the bits of the last
+// one in registers); once the piece is done, each lane queues that unit's bits and puts its other
+// marked units on a per-warp leftover list, recomputed 32 at a time, so the warp votes and
+// diverges once per piece instead of after every unit, and never waits on a few lanes' units.
 template <int NB, int K, int NT>
 __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
     using G = Geo<K>;
@@ -793,7 +795,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             // warp-uniform FULL and block-uniform C2 select the loop body, so the range masks and the
             // group-2 popcounts are not issued (as predicated code) where they cannot apply
             uint32_t pend;                                // units of this piece with survivors
-            uint4 save;                                   // bits of its first one
+            uint4 save;                                   // bits of the last one
             if (full)
                 pend = c2_live ? piece_units<NB, U, true, true>(rb, lane, s, e, c, save)
                                : piece_units<NB, U, true, false>(rb, lane, s, e, c, save);
