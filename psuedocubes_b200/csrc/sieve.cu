@@ -760,8 +760,6 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const bool active = rel < nv_item;
             VRec rec{};
             if (active) rec = a.rec[va + rel];
-            // the record of the next round is prefetched into L1 (no registers held across the round)
-            if (r + 1 < r_end && rel + 32 < nv_item) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.rec + va + rel + 32));
             // warp-uniform: all 32 rows exist and cover the whole block
             const bool full = r * 32 >= full_lo && r * 32 + 32 <= full_hi;
             // piece as bits of the block (an inactive lane's zeroed record gives an empty piece)
