@@ -263,12 +263,13 @@ class WindowBatch:
 
     def assemble(self, counts: np.ndarray, geometry: np.ndarray, records: np.ndarray) -> list[dict[str, Any]]:
         """Per-window results from the raw counters, envelope sizes and output records of a run
-        (host work only).  Counters of all windows are reduced in a few array passes; only
-        windows that emitted values touch them one by one."""
+        (host work only).  The subtile fields of all windows are formed in a few array passes and
+        one pass over the subtiles; only subtiles that emitted values are visited one by one."""
         n, nt = len(self.windows), self.ntiles
         tb = self.tile_base.astype(np.int64)
-        ngs = np.array([self.families[self._family_of[i]].ng for i in range(n)], dtype=np.int64)
-        tile_ng = np.repeat(ngs, np.diff(tb))
+        per = np.diff(tb)
+        ngs = [self.families[self._family_of[i]].ng for i in range(n)]
+        tile_ng = np.repeat(np.array(ngs, dtype=np.int64), per)
         at = np.arange(nt)
         emitted = counts[at, tile_ng + 1]
         if np.any(counts[at, tile_ng + 2]):
@@ -281,53 +282,60 @@ class WindowBatch:
         order = np.argsort(tile, kind='stable')
         tile_sorted = tile[order]
         lo_limb, hi_limb = records[order, 0], records[order, 1] & np.uint64(0xFFFFFFFF)
-        cuts = np.searchsorted(tile_sorted, np.arange(nt + 1))
+        cuts = np.searchsorted(tile_sorted, np.arange(nt + 1)).tolist()
+        # subtile bounds: window first + k * width, the last one ending at the window's end
+        owner = np.repeat(np.arange(n), per)
+        firsts = [w.first for w in self.windows]
+        ends = [w.end for w in self.windows]
+        if max(ends, default=0) + max(self.widths, default=0) < 2**63:
+            f64, w64 = np.array(firsts, dtype=np.int64)[owner], np.array(self.widths, dtype=np.int64)[owner]
+            sub_first = f64 + (at - tb[owner]) * w64
+            sub_end = np.minimum(sub_first + w64, np.array(ends, dtype=np.int64)[owner])
+            first_l, end_l = sub_first.tolist(), sub_end.tolist()
+        else:                                             # bounds beyond 64 bits: plain integers
+            first_l, end_l = [], []
+            for w, wd in zip(self.windows, self.widths):
+                for a in range(w.first, w.end, wd):
+                    first_l.append(a)
+                    end_l.append(min(a + wd, w.end))
+        starts, stops = list(map(str, first_l)), list(map(str, end_l))
         valid = counts[:, 0].tolist()
         emitted_list = emitted.tolist()
         sums = np.add.reduceat(counts, tb[:-1], axis=0).tolist() if nt else [[0] * self.stride] * n
         gu, gv = geometry[:, 0].tolist(), geometry[:, 1].tolist()
-        # group populations as Python lists, one conversion per family over the family's subtiles
-        family_rows: dict[int, list] = {}
-        where: list[tuple[list, int]] = []
+        cart = [a * b for a, b in zip(gu, gv)]
+        # group populations per subtile, one conversion per family over the family's subtiles
+        groups: list = [None] * nt
+        fam_of_tile = np.repeat(np.array(self._family_of, dtype=np.int64), per)
         for f in sorted(set(self._family_of)):
-            members = [i for i in range(n) if self._family_of[i] == f]
-            sel = np.concatenate([np.arange(tb[i], tb[i + 1]) for i in members])
-            family_rows[f] = counts[sel, 1:self.families[f].ng + 1].tolist()
-        offsets = {f: 0 for f in family_rows}
-        for i in range(n):
-            f = self._family_of[i]
-            where.append((family_rows[f], offsets[f]))
-            offsets[f] += int(tb[i + 1] - tb[i])
+            idx = np.nonzero(fam_of_tile == f)[0]
+            for t, row in zip(idx.tolist(), counts[idx, 1:self.families[f].ng + 1].tolist()):
+                groups[t] = row
+        # emitted values: sorted per subtile, checked against the subtile, digested
+        digests = [EMPTY_DIGEST] * nt
+        values_of: dict[int, list[int]] = {}
+        for t in np.nonzero(emitted)[0].tolist():
+            k0, k1 = cuts[t], cuts[t + 1]
+            tile_values = sorted(int(a) | int(b) << 64 for a, b in zip(lo_limb[k0:k1].tolist(), hi_limb[k0:k1].tolist()))
+            i = int(owner[t])
+            c, first, end = self.configs[i], first_l[t], end_l[t]
+            if any(not first <= c.canonical(x)[1] < end for x in tile_values):
+                raise ArithmeticError('output assigned to wrong subtile')
+            digests[t] = digest([str(x) for x in tile_values])
+            values_of.setdefault(i, []).extend(tile_values)
+        scopes = [{'first': a, 'end': b, 'valid_focused_candidates': v, 'group_survivors': g, 'local_survivors': e,
+                   'output_sha256': d}
+                  for a, b, v, g, e, d in zip(starts, stops, valid, groups, emitted_list, digests)]
+        tbl, sizes = tb.tolist(), self.sizes.tolist()
         out = []
         for i, (w, c) in enumerate(zip(self.windows, self.configs)):
-            t0, t1, ng = int(tb[i]), int(tb[i + 1]), int(ngs[i])
-            width = self.widths[i]
-            rows_f, at0 = where[i]
-            group_rows = rows_f[at0:at0 + t1 - t0]
-            firsts = range(w.first, w.end, width)
-            digests, values = [EMPTY_DIGEST] * (t1 - t0), []
-            for t in range(t0, t1):
-                if not emitted_list[t]:
-                    continue
-                k0, k1 = int(cuts[t]), int(cuts[t + 1])
-                tile_values = sorted(int(a) | int(b) << 64 for a, b in zip(lo_limb[k0:k1].tolist(), hi_limb[k0:k1].tolist()))
-                first = w.first + (t - t0) * width
-                end = min(first + width, w.end)
-                if any(not first <= c.canonical(x)[1] < end for x in tile_values):
-                    raise ArithmeticError('output assigned to wrong subtile')
-                digests[t - t0] = digest([str(x) for x in tile_values])
-                values.extend(tile_values)
+            t0, t1, ng = tbl[i], tbl[i + 1], ngs[i]
+            values = values_of.get(i, [])
             hits = verify_values(c, values) if values else []
-            starts = list(map(str, firsts))
-            ends = starts[1:] + [str(w.end)]
-            scopes = [{'first': a, 'end': b, 'valid_focused_candidates': v, 'group_survivors': g, 'local_survivors': e,
-                       'output_sha256': d}
-                      for a, b, v, g, e, d in zip(starts, ends, valid[t0:t1], group_rows, emitted_list[t0:t1], digests)]
-            us, vs = gu[t0:t1], gv[t0:t1]
-            row = dict(status='PASS', host_verified=True, focus_u=int(self.sizes[2 * i]),
-                       focus_v=int(self.sizes[2 * i + 1]), cartesian_opportunities=sum(a * b for a, b in zip(us, vs)),
+            row = dict(status='PASS', host_verified=True, focus_u=int(sizes[2 * i]),
+                       focus_v=int(sizes[2 * i + 1]), cartesian_opportunities=sum(cart[t0:t1]),
                        valid_focused_candidates=sum(valid[t0:t1]), genuine_cubes=len(values) - len(hits),
-                       local_survivors=len(values), cube_checks=len(values), subtile_scopes=scopes,
+                       local_survivors=len(values), cube_checks=len(values), subtile_scopes=scopes[t0:t1],
                        filter_groups=self.families[self._family_of[i]].filter_groups,
                        group_survivors=sums[i][1:ng + 1] if t1 > t0 else [0] * ng,
                        all_values=[str(x) for x in values], cpu_confirmed_hits=hits, overflow_splits=[],
