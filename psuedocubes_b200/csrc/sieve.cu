@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const uint64_t tile = tile_base + slot;
             if (tile >= seg_tiles_end) return;            // v outside the subtile geometry (reported by k_vprep)
             const uint32_t uidx = ent >> 20;
-            const uint64_t cr = a.cres[va + (ent & 0xFFFFFu)];
+            const uint64_t cr = __ldcg(a.cres + va + (ent & 0xFFFFFu));
             for (uint32_t t = 0; t < nch; ++t) {
                 const uint32_t vr = (uint32_t)(cr >> (16 * t)) & 0xFFFFu;
                 int32_t m = (int32_t)ures[t * G::UB + uidx] - (int32_t)vr;
@@ -729,7 +729,11 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const uint32_t rel = ent & 0xFFFFFu, u = (ent >> 20) & 0xFu;
             uint32_t slot = ent >> 24;
             if (mine) {
-                const VRec rr = a.rec[va + rel];
+                VRec rr;                                  // from L2, like the round's record
+                const uint4 *src = (const uint4 *)(a.rec + va + rel);
+                const uint4 h0 = __ldcg(src), h1 = __ldcg(src + 1);
+                memcpy(&rr, &h0, 16);
+                memcpy((char *)&rr + 16, &h1, 16);
                 if (slot == 255u) {
                     const uint64_t lt = local_tile(rr.v, S.v_first, S.width, S.ntiles);
                     slot = lt < S.ntiles ? (uint32_t)(S.tile_base + lt - tile_base) : NO_SLOT;
@@ -759,7 +763,12 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const uint32_t rel = r * 32 + lane;
             const bool active = rel < nv_item;
             VRec rec{};
-            if (active) rec = a.rec[va + rel];
+            if (active) {                                 // read once per block: cached in L2 only
+                const uint4 *src = (const uint4 *)(a.rec + va + rel);
+                const uint4 h0 = __ldcg(src), h1 = __ldcg(src + 1);
+                memcpy(&rec, &h0, 16);
+                memcpy((char *)&rec + 16, &h1, 16);
+            }
             // warp-uniform: all 32 rows exist and cover the whole block
             const bool full = r * 32 >= full_lo && r * 32 + 32 <= full_hi;
             // piece as bits of the block (an inactive lane's zeroed record gives an empty piece)
