@@ -36,9 +36,9 @@ BATCHES_TOTAL = 108298517
 LEASE_BATCHES = 256
 OPS_PER_POSITION = 0.53071   # algorithmic 32-bit lane-ops per focused position (3W + 18S1 + 12T + 24Nv)
 # DRAM bytes per focused position of k_match from one ncu capture of a full lease (first seeded
-# lease; dram__bytes_read.sum + dram__bytes_write.sum of the k_match launch: 715,479,808 + 28,950,272
+# lease; dram__bytes_read.sum + dram__bytes_write.sum of the k_match launch: 716,375,552 + 29,217,280
 # bytes over 274,244,194,629 positions; profiles/)
-DRAM_BYTES_PER_POSITION = (715_479_808 + 28_950_272) / 274244194629
+DRAM_BYTES_PER_POSITION = (716_375_552 + 29_217_280) / 274244194629
 
 
 def seeded_first_batch() -> int:
