@@ -75,6 +75,35 @@ def test_every_workload_prime_matches_oracle(runtime, engine, oracle, oracle619)
     assert sum(row['valid_focused_candidates'] for row in rows) > 10**9
 
 
+@pytest.mark.parametrize('width', [1, 5])
+def test_fine_subtiles_match_oracle(runtime, engine, oracle, width):
+    """Subtiles so narrow that one work item spans hundreds of them: a piece's further marked
+    units wait on the leftover list with subtile slots past its 8-bit field, which are recomputed
+    from v, and the survivor counters go to global memory past the shared slots.  At p = 31 the
+    bitset filters (q = 5, 11, 17, 23, 29, none 1 mod 3) keep every position, so nearly every unit
+    of a piece goes through the leftover list.  The oracle's masked batch takes at most 64
+    subtiles, so it runs over consecutive 64-subtile stretches of the window; every subtile's scope
+    and the window's totals are checked against them."""
+    w = Window(31, 0, 3627, 0, 100000, 266, 3627)
+    batch = engine.plan([w], width=width, output_cap=1 << 16)
+    batch.run()
+    row = batch.results()[0]
+    batch.close()
+    g = oracle.Geometry(w.p, w.lo, w.hi, w.A, w.B)
+    fa, fb = oracle.OracleFocus(g, 'A'), oracle.OracleFocus(g, 'B')
+    parts = [oracle.batch(g, fa, fb, a, min(a + 64 * width, w.end), width=width, output_cap=1 << 16)
+             for a in range(w.first, w.end, 64 * width)]
+    assert len(row['subtile_scopes']) == -(-w.end // width) > 255
+    assert row['subtile_scopes'] == [sc for part in parts for sc in part['subtile_scopes']]
+    for key in ('cartesian_opportunities', 'valid_focused_candidates', 'genuine_cubes', 'local_survivors',
+                'cube_checks'):
+        assert row[key] == sum(part[key] for part in parts), key
+    assert row['group_survivors'] == [sum(col) for col in zip(*(part['group_survivors'] for part in parts))]
+    assert row['filter_groups'] == parts[0]['filter_groups']
+    assert sorted(int(n) for n in row['all_values']) == sorted(int(n) for part in parts for n in part['all_values'])
+    assert row['local_survivors'] > 0
+
+
 def test_subtile_width_does_not_change_window_results(runtime, engine):
     windows = seeded_windows(24, seed=7, span_exp=(6.0, 9.3))
     base = None
