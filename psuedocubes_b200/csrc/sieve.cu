@@ -1840,10 +1840,12 @@ int multi_eager(pc_ctx *ctx, pc_multi *m, pc_stats *stats) {
     Engine &E = m->E;
     int launches = 0;
     PC_CHECK(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
-    int rc = winbatch_count(ctx, m->wb);
-    if (!rc) rc = winbatch_emit(ctx, m->wb, m->d_lists);
+    // pc_multi_create ran the count pass and its scan to size the lists; the unit counts, offsets
+    // and kept words it left depend only on the windows, so the eager run goes straight to the emit
+    // pass (a graph replay still runs both passes)
+    int rc = winbatch_emit(ctx, m->wb, m->d_lists);
     if (rc) return rc;
-    launches += 5;
+    launches += 1;
     PC_CHECK(ctx, cudaEventRecord(ctx->ev[5], ctx->stream));
     rc = engine_eager(E, &launches);
     if (rc) return rc;
