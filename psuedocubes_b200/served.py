@@ -356,7 +356,7 @@ class ServedLoop:
                     chosen.append((w, win))
             return chosen
 
-        def absorb(step: list[tuple[Work, Window]], outcome: tuple) -> None:
+        def absorb(step: list[tuple[Work, Window]], outcome: tuple) -> list[Work]:
             nonlocal positions_total
             counts, records, stats, ngs = outcome
             tiles = (records[:, 1] >> np.uint64(32)).astype(np.int64) if len(records) else np.zeros(0, np.int64)
@@ -383,9 +383,15 @@ class ServedLoop:
                                    **{k: stats.get(k, 0) for k in ('kernel_ms', 'total_ms', 'window_ms', 'bounds_ms',
                                                                    'u_entries', 'v_entries', 'launches', 'h2d_bytes',
                                                                    'd2h_bytes')}))
-            for w in [w for w in active if not w.pending and not w.outstanding]:
+            done = [w for w in active if not w.pending and not w.outstanding]
+            for w in done:                                # their memory is free for the next admission
                 active.remove(w)
                 self.reserved -= w.reserved
+            return done
+
+        def finish(done: list[Work]) -> None:
+            """Host verification and results of the requests a step completed."""
+            for w in done:
                 res = _finish(w)
                 res['cube_control'] = w.control.result()
                 if res['cube_control'] != res['genuine_cubes']:
@@ -408,7 +414,16 @@ class ServedLoop:
                     if step:
                         inflight = (pool.submit(self._device_step, [w for _, w in step]), step)
                         step = []
-                    absorb(prev, outcome)
+                    done = absorb(prev, outcome)
+                    if not inflight:
+                        # nothing queued on the device: refill it before the host verifies the
+                        # requests this step completed
+                        admit()
+                        step = compose()
+                        if step:
+                            inflight = (pool.submit(self._device_step, [w for _, w in step]), step)
+                            step = []
+                    finish(done)
                 if step:
                     inflight = (pool.submit(self._device_step, [w for _, w in step]), step)
                 elif not inflight and arrivals and not active and not waiting:
