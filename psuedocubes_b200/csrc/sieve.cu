@@ -81,6 +81,7 @@ struct FamDev {
     uint32_t cq[PC_MAX_CHEAP], caq[PC_MAX_CHEAP], cbq[PC_MAX_CHEAP], cbits_off[PC_MAX_CHEAP];
     ModQ cmq[PC_MAX_CHEAP];
     uint8_t bgroup[16];              // group ended by filter idx (0 = none), idx < NB + nch
+    uint32_t cqg[PC_MAX_CHEAP];      // cheap-tier filter t: q | the group it ends (bgroup[NB + t]) << 16
     const uint32_t *pat;
     const uint32_t *bits;
     const FiltC *fcs;
@@ -672,11 +673,11 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             const uint32_t uidx = ent >> 20;
             const uint64_t cr = __ldcg(a.cres + va + (ent & 0xFFFFFu));
             for (uint32_t t = 0; t < nch; ++t) {
-                const uint32_t vr = (uint32_t)(cr >> (16 * t)) & 0xFFFFu;
+                const uint32_t vr = (uint32_t)(cr >> (16 * t)) & 0xFFFFu, qg = F.cqg[t];
                 int32_t m = (int32_t)ures[t * G::UB + uidx] - (int32_t)vr;
-                if (m < 0) m += (int32_t)F.cq[t];
+                if (m < 0) m += (int32_t)(qg & 0xFFFFu);
                 if (!((cbits[t * CBW + (m >> 5)] >> (m & 31)) & 1u)) return;
-                const uint32_t g = F.bgroup[NB + t];
+                const uint32_t g = qg >> 16;
                 if (g) {
                     if (slot < a.tmax) atomicAdd(cnt_s + slot * cstride + g, 1u);
                     else atomicAdd((unsigned long long *)&a.counts[tile * a.stride + g], 1ull);
@@ -738,10 +739,10 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
                     const uint64_t lt = local_tile(rr.v, S.v_first, S.width, S.ntiles);
                     slot = lt < S.ntiles ? (uint32_t)(S.tile_base + lt - tile_base) : NO_SLOT;
                 }
-                acc = rows[(uint32_t)rr.row[0] * U + u];
+                acc = lds128(rows_addr + ((uint32_t)rr.row[0] * U + u) * 16);
 #pragma unroll
                 for (int f = 1; f < NB; ++f) {
-                    const uint4 w = rows[(uint32_t)rr.row[f] * U + u];
+                    const uint4 w = lds128(rows_addr + ((uint32_t)rr.row[f] * U + u) * 16);
                     acc.x &= w.x;
                     acc.y &= w.y;
                     acc.z &= w.z;
@@ -771,9 +772,13 @@ __global__ void __launch_bounds__(NT, 1) k_match(const MatchArgs a) {
             }
             // warp-uniform: all 32 rows exist and cover the whole block
             const bool full = r * 32 >= full_lo && r * 32 + 32 <= full_hi;
-            // piece as bits of the block (an inactive lane's zeroed record gives an empty piece)
-            const int32_t s = active ? max((int32_t)(rec.left - block_u0), 0) : 0;
-            const int32_t e = max(min((int32_t)(rec.right - block_u0), (int32_t)G::UB), s);
+            // piece as bits of the block, needed only where a row of the round covers part of it
+            // (an inactive lane's zeroed record gives an empty piece)
+            int32_t s = 0, e = (int32_t)G::UB;
+            if (!full) {
+                s = active ? max((int32_t)(rec.left - block_u0), 0) : 0;
+                e = max(min((int32_t)(rec.right - block_u0), (int32_t)G::UB), s);
+            }
             const bool moved = active && rec.v >= t_hi;
             if (__any_sync(0xffffffffu, moved)) {
                 flush();
@@ -1216,6 +1221,7 @@ FamDev fam_dev(const pc_filters *f, uint32_t nb, uint32_t nch) {
     }
     for (uint32_t idx = 0; idx < 16; ++idx)
         d.bgroup[idx] = (uint8_t)(idx < f->nres && ((idx & 3) == 3 || idx + 1 == f->nres) ? idx / 4 + 1 : 0);
+    for (uint32_t t = 0; t < nch; ++t) d.cqg[t] = d.cq[t] | (uint32_t)d.bgroup[nb + t] << 16;
     d.pat = f->d_pat;
     d.bits = f->d_bits;
     d.fcs = f->d_fcs;
